@@ -1,0 +1,207 @@
+/*
+ * pfg.h - C ABI of the B200 SSSP / A* engine (libpfg_b200.so).
+ *
+ * This is the drop-in boundary. The reference hides its CUDA code behind the
+ * C++ class `GpuSolver` (reference: include/gpu_sssp.h:97-120, implemented in
+ * src/gpu_sssp.cu:61-569 and src/gpu_device.cu:11-160). Here the same
+ * operations are exported as plain C functions over an opaque handle, with
+ * plain pointers and sizes and an integer status instead of exceptions and
+ * exit(). The C++ `GpuSolver` (include/gpu_sssp.h, gpu_solver.cpp) and the
+ * Python package are thin layers over these symbols.
+ *
+ * Conventions
+ *  - Every function returns a pfg_status; PFG_OK is 0. On failure
+ *    pfg_last_error() returns a human readable message for the calling
+ *    thread.
+ *  - Pointers named h_* are host memory, d_* are device memory of the
+ *    solver's device.
+ *  - Distances are uint32 with PFG_INF = 0xFFFFFFFF for "unreachable", parents
+ *    are uint32 with PFG_NO_PARENT = 0xFFFFFFFF. The packed state word of a
+ *    vertex is (dist << 32) | parent (reference: src/gpu_kernels.cuh:11-13).
+ *  - A solver is not thread safe: one host thread drives one solver, as in
+ *    the reference (src/gpu_sssp.cu:92, one stream per solver, no locking).
+ */
+#ifndef PFG_H_
+#define PFG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PFG_API __attribute__((visibility("default")))
+#else
+#define PFG_API
+#endif
+
+#define PFG_ABI_VERSION 1
+#define PFG_INF 0xFFFFFFFFu
+#define PFG_NO_PARENT 0xFFFFFFFFu
+
+typedef enum pfg_status {
+    PFG_OK = 0,
+    PFG_ERR_INVALID_ARGUMENT = 1, /* bad batch size, source, target, option  */
+    PFG_ERR_INVALID_GRAPH = 2,    /* CSR not well formed (see pfg_create)     */
+    PFG_ERR_OUT_OF_MEMORY = 3,    /* device memory precheck or cudaMalloc     */
+    PFG_ERR_NOT_CONVERGED = 4,    /* device round cap reached                  */
+    PFG_ERR_DEVICE_TIMEOUT = 5,   /* a bounded device-side wait gave up        */
+    PFG_ERR_CUDA = 6,             /* any other CUDA runtime error              */
+    PFG_ERR_NO_DEVICE = 7,        /* no CUDA device / ordinal out of range     */
+    PFG_ERR_CAPACITY = 8          /* a fixed-size resource is exhausted        */
+} pfg_status;
+
+/* Enum values follow the declaration order of the reference's enums
+ * (include/gpu_sssp.h:10-35) so that a static_cast maps one onto the other. */
+enum pfg_algo { PFG_ALGO_NAIVE = 0, PFG_ALGO_FRONTIER = 1, PFG_ALGO_DELTA = 2 };
+enum pfg_mapping { PFG_MAP_THREAD = 0, PFG_MAP_WARP = 1, PFG_MAP_HYBRID = 2 };
+enum pfg_atomic { PFG_ATOMIC_MIN_RBA = 0, PFG_ATOMIC_CAS_RBA = 1, PFG_ATOMIC_MIN_NOCHECK = 2 };
+enum pfg_compaction { PFG_COMPACT_WARP_ATOMIC = 0, PFG_COMPACT_PREFIX_SCAN = 1 };
+/* Schedule policy for Delta-stepping (extension; no reference counterpart). */
+enum pfg_policy_kind { PFG_POLICY_FIXED = 0, PFG_POLICY_LEARNED = 1 };
+
+/* Mirrors GpuOptions (reference: include/gpu_sssp.h:42-52) plus `policy`. */
+typedef struct pfg_options {
+    int32_t algo;        /* enum pfg_algo, default PFG_ALGO_DELTA                 */
+    int32_t mapping;     /* enum pfg_mapping, default PFG_MAP_HYBRID              */
+    int32_t atomic;      /* enum pfg_atomic, default PFG_ATOMIC_MIN_RBA           */
+    uint32_t delta;      /* 0 = automatic, round(32 * avgW / avgDeg)              */
+    int32_t block_size;  /* threads per CTA; invalid values fall back to 256      */
+    uint32_t sync_every; /* accepted for compatibility; convergence is detected
+                            on the device, so the host synchronizes once per run */
+    int32_t compaction;  /* enum pfg_compaction (Frontier only)                   */
+    int32_t policy;      /* enum pfg_policy_kind (Delta-stepping only)            */
+} pfg_options;
+
+/* Mirrors GpuStats (reference: include/gpu_sssp.h:55-65) plus `rounds`. */
+typedef struct pfg_stats {
+    uint64_t edges_scanned;  /* real (non padding) arcs examined                */
+    uint64_t atomics_issued; /* 64-bit atomicMin / atomicCAS on the state        */
+    uint64_t updates;        /* relaxations that lowered a distance             */
+    uint64_t pushes;         /* queue insertions                                 */
+    uint32_t iterations;     /* device rounds with a non-empty input             */
+    uint32_t host_syncs;     /* host waits inside the run (1: the final one)    */
+    uint32_t launches;       /* kernel launches issued by the run                */
+    uint32_t buckets;        /* Delta-stepping buckets processed                 */
+    uint32_t delta;          /* Delta of the first bucket (0 unless Delta-step)  */
+    uint32_t rounds;         /* device rounds executed (barrier epochs)          */
+} pfg_stats;
+
+typedef struct pfg_solver pfg_solver;
+
+/* ---- solver life cycle (reference: GpuSolver::GpuSolver / ~GpuSolver,
+ *      src/gpu_sssp.cu:107-200) ----
+ * row_offsets[n+1], col_indices[m], weights[m]: host CSR. Rows must be sorted
+ * by weight (the reference's buildCSR sorts each row by (w, dst),
+ * src/graph.cpp:57-74); weights must be >= 1; col < n; row_offsets
+ * non-decreasing with row_offsets[0] = 0 and row_offsets[n] = m.
+ * x, y: optional vertex coordinates (both NULL or both of length n) for the
+ * A* heuristic; h_scale is CSRGraph::hScale (0 disables the heuristic).
+ * avg_w / avg_deg feed the automatic Delta (reference: src/gpu_sssp.cu:202-206).
+ * max_batch: largest number of sources one run may use; max_batch * n must be
+ * < 2^32 (reference: src/gpu_sssp.cu:108). */
+PFG_API pfg_status pfg_create(const uint32_t* row_offsets, const uint32_t* col_indices,
+                      const uint32_t* weights, const double* x, const double* y,
+                      uint32_t n, uint32_t m, double h_scale, double avg_w,
+                      double avg_deg, uint32_t max_batch, pfg_solver** out);
+/* Same, on an explicit CUDA device ordinal (the reference always uses 0). */
+PFG_API pfg_status pfg_create_on_device(const uint32_t* row_offsets, const uint32_t* col_indices,
+                                const uint32_t* weights, const double* x, const double* y,
+                                uint32_t n, uint32_t m, double h_scale, double avg_w,
+                                double avg_deg, uint32_t max_batch, int32_t device,
+                                pfg_solver** out);
+PFG_API void pfg_destroy(pfg_solver* s);
+
+/* Accessors (reference: GpuSolver::uploadMs / deviceBytes / autoDelta,
+ * src/gpu_sssp.cu:540-543). */
+PFG_API double pfg_upload_ms(const pfg_solver* s);
+PFG_API uint64_t pfg_device_bytes(const pfg_solver* s);
+PFG_API uint32_t pfg_auto_delta(const pfg_solver* s);
+PFG_API uint32_t pfg_num_vertices(const pfg_solver* s);
+PFG_API uint32_t pfg_max_batch(const pfg_solver* s);
+/* cudaStream_t of the solver, as void*, so callers can record events on it. */
+PFG_API void* pfg_stream(const pfg_solver* s);
+
+/* ---- one run (reference: GpuSolver::Impl::run, src/gpu_sssp.cu:461-534) ----
+ * Shortest paths from k sources h_srcs[0..k) (1 <= k <= max_batch), all in
+ * one device launch; instance i owns state words [i*n, (i+1)*n).
+ * astar != 0: point-to-point A* from h_srcs[0] to dst (k must be 1); keys are
+ * dist + h(v) and every relaxation is pruned at dist[dst] (reference:
+ * src/gpu_kernels.cuh:178-179).
+ * h_state_out (nullable): receives k*n packed state words.
+ * ms_out (nullable): device time of initialisation + relaxation measured with
+ * CUDA events on the solver's stream (the reference's r.ms, which excludes
+ * copy-back, src/gpu_sssp.cu:478-502).
+ * Errors: PFG_ERR_INVALID_ARGUMENT for k == 0, k > max_batch, a source >= n,
+ * dst >= n when astar, or astar with k != 1 (reference: src/gpu_sssp.cu:463-465).
+ * opt == NULL means default options. Like the reference, Naive with k > 1
+ * silently runs Delta-stepping (src/gpu_sssp.cu:466). */
+PFG_API pfg_status pfg_run(pfg_solver* s, const uint32_t* h_srcs, uint32_t k, int32_t astar,
+                   uint32_t dst, const pfg_options* opt, pfg_stats* stats_out,
+                   uint64_t* h_state_out, float* ms_out);
+
+/* Same run with the sources already on the device (d_srcs, k entries) and no
+ * host synchronisation: work is enqueued on the solver's stream and the call
+ * returns immediately. Results stay in the solver's state buffer
+ * (pfg_state_device). Statistics and errors of an asynchronous run are read
+ * with pfg_finish(). */
+PFG_API pfg_status pfg_run_async(pfg_solver* s, const uint32_t* d_srcs, uint32_t k, int32_t astar,
+                         uint32_t dst, const pfg_options* opt);
+/* Waits for the last asynchronous run, returns its status and statistics. */
+PFG_API pfg_status pfg_finish(pfg_solver* s, pfg_stats* stats_out);
+/* Device pointer to the k*n packed state words of the last run. */
+PFG_API const uint64_t* pfg_state_device(const pfg_solver* s);
+
+/* Copies state words [first, first+count) of the last run to host memory. */
+PFG_API pfg_status pfg_copy_state(pfg_solver* s, uint64_t first, uint64_t count, uint64_t* h_out);
+
+/* Reconstructs the path src -> dst of instance `inst` of the last run on the
+ * device by following parent pointers (reference: reconstructPath,
+ * src/cpu_sssp.cpp:124-135). path_len_out = 0 when dst is unreachable or the
+ * parent chain is broken. Fails with PFG_ERR_CAPACITY when the path has more
+ * than cap vertices. */
+PFG_API pfg_status pfg_extract_path(pfg_solver* s, uint32_t inst, uint32_t src, uint32_t dst,
+                            uint32_t* h_path, uint32_t cap, uint32_t* path_len_out);
+
+/* ---- device information (reference: gpuQueryDevice / gpuWarmup /
+ *      gpuTransferStudy, src/gpu_device.cu:39-160) ---- */
+typedef struct pfg_device_info {
+    int32_t ok;
+    char name[256];
+    int32_t cc_major, cc_minor, sm_count, clock_mhz, mem_clock_mhz, bus_width;
+    int32_t driver_version, runtime_version, max_threads_per_sm, warp_size;
+    uint64_t global_mem, shared_per_block, l2_bytes;
+    double peak_bandwidth_gbs;
+} pfg_device_info;
+PFG_API pfg_status pfg_query_device(int32_t dev, pfg_device_info* out);
+PFG_API pfg_status pfg_warmup(void);
+
+typedef struct pfg_transfer_study {
+    double bytes, pageable_ms, pinned_ms, pinned_streams_ms;
+} pfg_transfer_study;
+PFG_API pfg_status pfg_transfer_study_run(const uint32_t* row_offsets, const uint32_t* col_indices,
+                                  const uint32_t* weights, uint32_t n, uint32_t m,
+                                  int32_t reps, pfg_transfer_study* out);
+
+/* ---- learned Delta policy (extension; no reference counterpart) ----
+ * The policy is a 12 -> 64 -> 64 -> 64 -> 8 fp32 MLP evaluated on the device
+ * at every bucket advance; its argmax picks the next bucket's Delta as one of
+ * {1/4, 1/2, 1, 2, 4, 8, 16, 64} x the automatic Delta. It only changes the
+ * schedule: distances and parents are the same as with a fixed Delta.
+ * pfg_set_policy loads a flat parameter image of pfg_policy_param_count()
+ * floats (layout: w1[64x12] b1 w2[64x64] b2 w3[64x64] b3 w4[8x64] b4
+ * in_mean[12] in_scale[12]). */
+PFG_API pfg_status pfg_set_policy(pfg_solver* s, const float* params, uint64_t count);
+PFG_API uint64_t pfg_policy_param_count(void);
+
+/* ---- errors ---- */
+PFG_API const char* pfg_last_error(void);
+PFG_API const char* pfg_status_string(pfg_status st);
+PFG_API int32_t pfg_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFG_H_ */

@@ -1,0 +1,225 @@
+// pfg_common.cuh - device-side types and helpers of the B200 SSSP / A* engine.
+//
+// Layout in HBM (one solver):
+//   adj    uint2[m_pad]   (col, w) pairs; every row starts on a 32-byte boundary
+//                         (4 arcs) and is padded with (self, 0xFFFFFFFF) arcs, so a
+//                         thread reads a whole row of a road graph in one sector
+//                         with 128-bit loads. Rows keep the caller's order, which
+//                         is sorted by weight (reference: src/graph.cpp:57-74), so
+//                         the light arcs (w <= Delta) of a row are a prefix.
+//   prow   u32[n+1]       padded row starts (multiples of 4).
+//   x, y   f64[n]         coordinates for the A* heuristic (optional).
+//   state  u64[K*n]       packed (dist << 32) | parent; one atomicMin updates both
+//                         and an equal distance keeps the smaller parent
+//                         (reference: src/gpu_kernels.cuh:11-13, 96-121).
+//   queues u32[K*n] x 5   near ping-pong, far ping-pong, R (heavy set).
+//   stamps u32[K*n] x 3   dedup words for near / far / R: an item is queued for
+//                         epoch E iff stamp == E. Epochs only grow, so nothing is
+//                         cleared between rounds or runs (the reference clears a
+//                         bitmask bit per item, src/gpu_kernels.cuh:124-132).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pfg {
+
+typedef uint32_t u32;
+typedef uint64_t u64;
+
+constexpr u32 INF32 = 0xFFFFFFFFu;
+constexpr u32 NO_PARENT = 0xFFFFFFFFu;
+constexpr u64 STATE_INIT = 0xFFFFFFFFFFFFFFFFull;  // (INF << 32) | NO_PARENT
+constexpr u32 PAD_W = 0xFFFFFFFFu;                 // weight of a padding arc
+constexpr u32 ROW_ALIGN = 4;                       // arcs per 32-byte sector
+
+// Phases of the persistent kernel's state machine.
+enum Phase : u32 {
+    PH_INIT = 0,   // state initialisation (grid-stride), then seeding
+    PH_LIGHT = 1,  // relax light arcs of the near queue
+    PH_SCAN = 2,   // bucket start: relax far items inside the new window, keep the rest
+    PH_HEAVY = 3,  // relax heavy arcs of the bucket's settled set R
+    PH_NAIVE = 4,  // Bellman-Ford sweep over all vertices (naive mode)
+    PH_COMPACT = 5,// prefix-sum compaction of the flagged next frontier
+    PH_DONE = 6
+};
+
+// Run modes (reference GpuAlgo, include/gpu_sssp.h:10-14).
+enum RunMode : int { MODE_NAIVE = 0, MODE_FRONTIER = 1, MODE_DELTA = 2 };
+
+// Queue counter slots in Ctl::cnt.
+enum CounterSlot : u32 { C_NEAR0 = 0, C_NEAR1 = 1, C_FAR0 = 2, C_FAR1 = 3, C_R = 4, C_COUNT = 8 };
+
+// Device status words (match pfg_status values).
+enum DevStatus : u32 { DS_OK = 0, DS_BAD_SOURCE = 1, DS_NOT_CONVERGED = 4, DS_TIMEOUT = 5 };
+
+// Control block in device memory. The part up to `persist` is rewritten by
+// the host before every run; the epoch counters below it carry over from run
+// to run so that stamp words never have to be cleared.
+struct Ctl {
+    // --- per run ---
+    u32 bar_count;     // grid barrier arrivals
+    u32 bar_gen;       // grid barrier generation
+    u32 phase;
+    u32 in_count;      // items in this round's input
+    u32 in_buf;        // near buffer read by a LIGHT round
+    u32 far_in;        // far pile scanned by a SCAN round
+    u32 far_out;       // far pile that receives pushes
+    u32 status;        // DevStatus
+    u32 rounds;        // barrier epochs so far
+    u32 iterations;    // rounds with a non-empty input
+    u32 buckets;
+    u32 round_cap;
+    u32 delta;         // Delta of the current bucket
+    u32 delta0;        // Delta of the first bucket
+    u32 heavy;         // nonzero when some arc is heavier than Delta
+    u32 changed;       // naive mode: some distance decreased this round
+    u32 naive_in;      // naive mode: which activity mask is read
+    u32 policy_calls;  // learned-policy decisions taken
+    u64 lo, hi;        // current bucket window [lo, hi) on the key
+    u64 far_min[2];    // smallest key pushed to each far pile
+    u32 cnt[C_COUNT];  // queue tails
+    unsigned long long stats[4];  // edges, atomics, updates, pushes
+    u32 bucket_near;   // items entering the current bucket (policy feature)
+    u32 bucket_rounds; // rounds spent in the current bucket (policy feature)
+    u64 bucket_edges;  // edges scanned up to the start of the bucket (policy feature)
+    u64 bucket_edges_acc;  // edges scanned so far, flushed every round when the policy runs
+    u32 flag_epoch;    // prefix-scan mode: stamp of the flagged vertices
+    u32 pad_run;
+    // --- persistent across runs ---
+    u32 persist;       // marker: everything below survives between runs
+    u32 near_epoch;    // stamp written by near pushes of the current round
+    u32 far_epoch;     // stamp of the far pile that receives pushes
+    u32 r_epoch;       // stamp of the current R set
+};
+
+// Learned Delta-policy network (3 hidden layers of 64, fp32).
+constexpr int POL_IN = 12;
+constexpr int POL_H = 64;
+constexpr int POL_OUT = 8;  // Delta multipliers, see kPolicyMult
+struct PolicyNet {
+    float w1[POL_H * POL_IN], b1[POL_H];
+    float w2[POL_H * POL_H], b2[POL_H];
+    float w3[POL_H * POL_H], b3[POL_H];
+    float w4[POL_OUT * POL_H], b4[POL_OUT];
+    float in_mean[POL_IN], in_scale[POL_IN];
+};
+
+// Parameters of one persistent run (passed by value as a __grid_constant__).
+struct RunParams {
+    const uint2* adj;
+    const u32* prow;
+    const double* x;
+    const double* y;
+    u32 n;
+    u32 maxw;          // largest real arc weight
+    double hscale;     // A* heuristic scale (0: h = 0)
+    double avg_w, avg_deg;
+    u32 m;
+    u32 k;             // instances (sources); instance i owns [i*n, (i+1)*n)
+    u32 total;         // k*n
+    const u32* srcs;   // device [k]
+    int astar;
+    u32 target;
+    double xt, yt;     // target coordinates (A*)
+    int use_h;         // heuristic enabled
+    u64* state;
+    u32* nearq[2];
+    u32* farq[2];
+    u32* rq;
+    u32* near_stamp;
+    u32* far_stamp;
+    u32* r_stamp;
+    u32* naive_mask[2];// naive mode: activity bitmasks [ceil(n/32)]
+    Ctl* ctl;
+    u32 delta;         // Delta of the first bucket (fixed-Delta mode: all buckets)
+    int mode;          // RunMode
+    int prefix_scan;   // 1: flag + scan compaction instead of queue pushes
+    int policy;        // 1: learned Delta policy picks each bucket's Delta
+    const PolicyNet* net;
+    u64 timeout_ns;    // bound on every device-side wait
+};
+
+// ---------------------------------------------------------------------------
+// Small device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u64 global_timer_ns() {
+    u64 t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// L2-coherent loads for data written by other CTAs during the same kernel.
+__device__ __forceinline__ u64 ld_state(const u64* p) { return __ldcg(p); }
+__device__ __forceinline__ u32 ld_cg(const u32* p) { return __ldcg(p); }
+__device__ __forceinline__ u32 vload(const u32* p) { return *(const volatile u32*)p; }
+__device__ __forceinline__ u64 vload64(const u64* p) { return *(const volatile u64*)p; }
+
+__device__ __forceinline__ u32 st_dist(u64 s) { return (u32)(s >> 32); }
+__device__ __forceinline__ u64 pack_state(u32 d, u32 p) { return ((u64)d << 32) | (u64)p; }
+
+// Admissible, consistent Euclidean heuristic. Same formula as the
+// reference's heuristicValue (include/heuristic.h:19-25) so that A* keys and
+// pruning follow the reference: h = floor(scale * |p(v) - p(t)| * (1 - 1e-9)),
+// clamped to 4e9.
+__host__ __device__ __forceinline__ u32 heuristic_value(double xv, double yv, double xt,
+                                                        double yt, double scale) {
+    const double dx = xv - xt, dy = yv - yt;
+    const double e = sqrt(dx * dx + dy * dy) * scale * (1.0 - 1e-9);
+    if (!(e > 0.0)) return 0u;
+    if (e >= 4.0e9) return 4000000000u;
+    return (u32)e;
+}
+
+// 64-bit update of the packed state. Returns true when the distance strictly
+// decreased (the caller then queues the vertex). An equal distance with a
+// smaller parent wins the atomicMin but returns false, as in the reference
+// (src/gpu_kernels.cuh:96-121).
+//   AM 0: read-before-atomic + atomicMin   (reference MinRBA)
+//   AM 1: read-before-atomic + CAS loop    (reference CasRBA)
+//   AM 2: blind atomicMin                  (reference MinNoCheck)
+template <int AM>
+__device__ __forceinline__ bool relax_state(u64* addr, u32 nd, u32 parent, u32& atomics) {
+    const u64 nv = pack_state(nd, parent);
+    if constexpr (AM == 2) {
+        atomics++;
+        const u64 old = atomicMin((unsigned long long*)addr, (unsigned long long)nv);
+        return st_dist(old) > nd;
+    } else {
+        u64 cur = ld_state(addr);
+        if (cur <= nv) return false;
+        if constexpr (AM == 0) {
+            atomics++;
+            const u64 old = atomicMin((unsigned long long*)addr, (unsigned long long)nv);
+            return st_dist(old) > nd;
+        } else {
+            // Lock-free: every failed CAS means another thread lowered the word.
+            while (true) {
+                atomics++;
+                const u64 old = atomicCAS((unsigned long long*)addr, (unsigned long long)cur,
+                                          (unsigned long long)nv);
+                if (old == cur) return st_dist(old) > nd;
+                cur = old;
+                if (cur <= nv) return false;
+            }
+        }
+    }
+}
+
+// Claims item i for epoch e: true exactly once per (i, e).
+__device__ __forceinline__ bool claim_stamp(u32* stamp, u32 i, u32 e) {
+    if (ld_cg(stamp + i) == e) return false;
+    return atomicExch(stamp + i, e) != e;
+}
+
+// Warp-aggregated append: one atomicAdd per group of converged lanes.
+__device__ __forceinline__ void queue_push(u32* q, u32* tail, u32 item) {
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    u32 base = 0;
+    if (lane == leader) base = atomicAdd(tail, (u32)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    q[base + __popc(mask & ((1u << lane) - 1u))] = item;
+}
+
+}  // namespace pfg

@@ -1,0 +1,802 @@
+// pfg_kernels.cu - persistent relaxation kernels of the B200 SSSP / A* engine.
+//
+// One cooperative launch runs a whole SSSP / A* / multi-source query: the
+// reference's host loops (runNaive / runFrontier / runDelta,
+// src/gpu_sssp.cu:257-456) become a state machine inside one kernel, so no
+// host round trip happens between relaxation rounds. Each round ends in a
+// bounded grid barrier; the CTA that arrives last runs the transition (queue
+// swaps, bucket advance, termination) while the others wait, and every CTA
+// reads the new control block after the barrier.
+//
+// Round kinds (reference counterparts):
+//   LIGHT  relax the light arcs (w <= Delta) of the near queue      relaxFrontierKernel<SEL_LIGHT / SEL_ALL>, src/gpu_kernels.cuh:207-288
+//   SCAN   bucket advance fused with the first light round: far items inside
+//          the new window are relaxed at once, the rest stay far  farMinKernel + farPartitionKernel, :386-436
+//   HEAVY  relax the heavy arcs (w > Delta) of R                    relaxFrontierKernel<SEL_HEAVY>
+//   NAIVE  Bellman-Ford sweep over all vertices with activity bits naiveRelaxKernel, :297-329
+//   COMPACT prefix-sum compaction of flagged vertices               cub::DeviceScan + scatterKernel, :376-383
+//
+// The window of the next bucket comes from the smallest key pushed to the far
+// pile (tracked per round with one atomicMin per CTA) instead of a separate
+// farMin pass; that value is a lower bound of every live far key, so buckets
+// are never skipped.
+#include "pfg_common.cuh"
+#include "pfg_kernels.h"
+
+#include <cstdio>
+
+namespace pfg {
+
+constexpr unsigned FULL = 0xFFFFFFFFu;
+constexpr u32 MAX_BS = 1024;
+constexpr u32 COOP_MIN = 32;  // hybrid mapping: rows with >= 32 selected arcs are CTA-cooperative
+
+enum Kind { K_LIGHT = 0, K_SCAN = 1, K_HEAVY = 2 };
+
+// Multipliers of the automatic Delta that the learned policy chooses from.
+__constant__ float kPolicyMult[POL_OUT] = {0.25f, 0.5f, 1.f, 2.f, 4.f, 8.f, 16.f, 64.f};
+
+// Control-block snapshot, refreshed in shared memory after every barrier.
+struct Snap {
+    u32 phase, in_count, in_buf, far_in, far_out, status, delta, heavy;
+    u32 near_epoch, far_epoch, r_epoch, naive_in, map_mode, flag_epoch;
+    u64 lo, hi;
+};
+
+struct Local {
+    u32 edges = 0, atomics = 0, updates = 0, pushes = 0;
+    u64 fmin = ~0ull;  // smallest key this thread pushed to the far pile this round
+};
+
+// Shared memory of the CTA-cooperative (scan-based) tier of the hybrid mapping.
+struct Coop {
+    u32 off[MAX_BS + 1];
+    u32 eb[MAX_BS];
+    u32 u[MAX_BS];
+    u32 du[MAX_BS];
+    u32 ib[MAX_BS];
+    u32 ub[MAX_BS];
+    u32 wsum[32];
+};
+
+// ---------------------------------------------------------------------------
+// Block-wide exclusive scan (warp shuffles + one pass over warp totals).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u32 block_exclusive_scan(u32 v, u32* wsum, u32& total) {
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const u32 nwarps = (blockDim.x + 31u) >> 5;
+    u32 x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(FULL, x, o);
+        if (lane >= (u32)o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        u32 t = lane < nwarps ? wsum[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 y = __shfl_up_sync(FULL, t, o);
+            if (lane >= (u32)o) t += y;
+        }
+        if (lane < nwarps) wsum[lane] = t;  // inclusive prefix of warp totals
+    }
+    __syncthreads();
+    total = wsum[nwarps - 1];
+    const u32 warp_base = warp ? wsum[warp - 1] : 0u;
+    __syncthreads();  // wsum may be reused right after
+    return warp_base + x - v;
+}
+
+__device__ __forceinline__ u64 block_min_u64(u64 v, u64* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const u64 y = __shfl_down_sync(FULL, v, o);
+        v = y < v ? y : v;
+    }
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    u64 r = ~0ull;
+    if (threadIdx.x == 0) {
+        const u32 nwarps = (blockDim.x + 31u) >> 5;
+        for (u32 i = 0; i < nwarps; ++i) r = red[i] < r ? red[i] : r;
+    }
+    return r;  // valid in thread 0
+}
+
+// ---------------------------------------------------------------------------
+// Heuristic and light/heavy split
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u32 h_of(const RunParams& p, u32 v) {
+    if (!p.use_h) return 0u;
+    return heuristic_value(p.x[v], p.y[v], p.xt, p.yt, p.hscale);
+}
+
+// First arc of [r0, r1) whose weight exceeds delta (rows are sorted by weight).
+__device__ __forceinline__ u32 light_end(const uint2* adj, u32 r0, u32 r1, u32 delta) {
+    u32 lo = r0, hi = r1;
+    while (lo < hi) {
+        const u32 mid = lo + ((hi - lo) >> 1);
+        if (__ldg(&adj[mid].y) <= delta) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Relaxation of one arc (u -> v, w) and queueing of the improved head.
+// ---------------------------------------------------------------------------
+template <bool ASTAR, int AM>
+__device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32 u, u32 du,
+                                          u32 ib, u32 ub, u32 v, u32 w, Local& L) {
+    if (w == PAD_W) return;
+    L.edges++;
+    const u64 nd = (u64)du + w;
+    if (nd >= INF32) return;
+    u64 key = nd;
+    if constexpr (ASTAR) {
+        key += h_of(p, v);
+        if (key >= ub) return;  // f(v) >= dist[target]: cannot improve the answer
+    }
+    const u32 gv = ib + v;
+    if (!relax_state<AM>(p.state + gv, (u32)nd, u, L.atomics)) return;
+    L.updates++;
+    Ctl* c = p.ctl;
+    if (p.prefix_scan) {  // flag only; the COMPACT round builds the next frontier
+        p.near_stamp[gv] = s.near_epoch;
+        L.pushes++;
+        return;
+    }
+    if (key < s.hi) {
+        if (claim_stamp(p.near_stamp, gv, s.near_epoch)) {
+            const u32 out = s.in_buf ^ 1u;
+            queue_push(p.nearq[out], &c->cnt[C_NEAR0 + out], gv);
+            L.pushes++;
+        }
+    } else {
+        if (claim_stamp(p.far_stamp, gv, s.far_epoch)) {
+            queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gv);
+            L.pushes++;
+        }
+        L.fmin = key < L.fmin ? key : L.fmin;
+    }
+}
+
+// Thread tier: one thread walks its own arcs [eb, ee) with 128-bit loads
+// (two arcs per load; rows start on 32-byte boundaries).
+template <bool ASTAR, int AM>
+__device__ __forceinline__ void relax_range_thread(const RunParams& p, const Snap& s, u32 u, u32 du,
+                                                   u32 ib, u32 ub, u32 eb, u32 ee, Local& L) {
+    const uint4* a4 = reinterpret_cast<const uint4*>(p.adj);
+    for (u32 e = eb & ~1u; e < ee; e += 2) {
+        const uint4 q = __ldg(a4 + (e >> 1));
+        if (e >= eb) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, q.x, q.y, L);
+        if (e + 1 < ee) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, q.z, q.w, L);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One round over an input array of items (state indices).
+// ---------------------------------------------------------------------------
+template <bool ASTAR, int AM, int MAP>
+__device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u32 count, int kind,
+                            Local& L, Coop& cs) {
+    const u32 BS = blockDim.x;
+    Ctl* c = p.ctl;
+    const bool split = s.heavy != 0;  // some arcs are heavier than Delta
+    for (u32 base = blockIdx.x * BS; base < count; base += gridDim.x * BS) {
+        const u32 idx = base + threadIdx.x;
+        u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, ub = INF32;
+        bool act = false;
+        if (idx < count) {
+            const u32 gi = ld_cg(in + idx);
+            const u32 inst = p.k > 1 ? gi / p.n : 0u;
+            ib = inst * p.n;
+            u = gi - ib;
+            du = st_dist(ld_state(p.state + gi));
+            act = du != INF32;
+            u64 key = du;
+            if constexpr (ASTAR) {
+                ub = st_dist(ld_state(p.state + ib + p.target));
+                if (act) {
+                    key += h_of(p, u);
+                    if (key >= ub) act = false;
+                }
+            }
+            if (kind == K_SCAN && act) {
+                if (key < s.lo) {
+                    act = false;  // settled in an earlier bucket (stale far entry)
+                } else if (key >= s.hi) {
+                    act = false;  // belongs to a later bucket: keep it far
+                    if (claim_stamp(p.far_stamp, gi, s.far_epoch)) {
+                        queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gi);
+                        L.pushes++;
+                    }
+                    L.fmin = key < L.fmin ? key : L.fmin;
+                }
+            }
+            if (act) {
+                const u32 r0 = __ldg(p.prow + u), r1 = __ldg(p.prow + u + 1);
+                if (kind == K_HEAVY) {
+                    eb = light_end(p.adj, r0, r1, s.delta);
+                    ee = r1;
+                } else {
+                    eb = r0;
+                    ee = split ? light_end(p.adj, r0, r1, s.delta) : r1;
+                    // R = vertices of this bucket that own real heavy arcs.
+                    if (split && ee < r1 && __ldg(&p.adj[ee].y) != PAD_W) {
+                        if (claim_stamp(p.r_stamp, gi, s.r_epoch)) {
+                            queue_push(p.rq, &c->cnt[C_R], gi);
+                            L.pushes++;
+                        }
+                    }
+                }
+                if (ee <= eb) act = false;
+            }
+        }
+
+        if constexpr (MAP == 0) {  // thread per item
+            if (act) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, eb, ee, L);
+        } else if constexpr (MAP == 1) {  // warp per item
+            const u32 lane = threadIdx.x & 31u;
+            unsigned ballot = __ballot_sync(FULL, act);
+            while (ballot) {
+                const int leader = __ffs(ballot) - 1;
+                ballot &= ballot - 1;
+                const u32 wu = __shfl_sync(FULL, u, leader), wdu = __shfl_sync(FULL, du, leader);
+                const u32 wib = __shfl_sync(FULL, ib, leader), wub = __shfl_sync(FULL, ub, leader);
+                const u32 web = __shfl_sync(FULL, eb, leader), wee = __shfl_sync(FULL, ee, leader);
+                for (u32 e = web + lane; e < wee; e += 32) {
+                    const uint2 a = __ldg(p.adj + e);
+                    relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, a.x, a.y, L);
+                }
+            }
+        } else {  // hybrid: short rows by their own thread, long rows CTA-cooperative
+            const bool big = act && (ee - eb) >= COOP_MIN && s.map_mode != 0;
+            if (act && !big) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, eb, ee, L);
+            if (__syncthreads_or(big)) {
+                u32 total = 0;
+                const u32 sz = big ? ee - eb : 0u;
+                const u32 off = block_exclusive_scan(sz, cs.wsum, total);
+                cs.off[threadIdx.x] = off;
+                cs.eb[threadIdx.x] = eb;
+                cs.u[threadIdx.x] = u;
+                cs.du[threadIdx.x] = du;
+                cs.ib[threadIdx.x] = ib;
+                cs.ub[threadIdx.x] = ub;
+                if (threadIdx.x == 0) cs.off[BS] = total;
+                __syncthreads();
+                for (u32 j = threadIdx.x; j < total; j += BS) {
+                    // owner = last slot with off <= j (slots of size 0 repeat offsets)
+                    u32 lo = 0, hi = BS;
+                    while (lo < hi) {
+                        const u32 mid = (lo + hi + 1) >> 1;
+                        if (cs.off[mid] <= j) lo = mid; else hi = mid - 1;
+                    }
+                    const u32 e = cs.eb[lo] + (j - cs.off[lo]);
+                    const uint2 a = __ldg(p.adj + e);
+                    relax_arc<ASTAR, AM>(p, s, cs.u[lo], cs.du[lo], cs.ib[lo], cs.ub[lo], a.x, a.y, L);
+                }
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Naive round: every vertex whose activity bit is set relaxes all its arcs
+// (Harish & Narayanan; reference naiveRelaxKernel, src/gpu_kernels.cuh:297-329).
+// ---------------------------------------------------------------------------
+template <bool ASTAR, int AM>
+__device__ void round_naive(const RunParams& p, const Snap& s, Local& L) {
+    u32* mask_in = p.naive_mask[s.naive_in];
+    u32* mask_out = p.naive_mask[s.naive_in ^ 1u];
+    Ctl* c = p.ctl;
+    const u32 stride = gridDim.x * blockDim.x;
+    const u32 lane = threadIdx.x & 31u;
+    // Each warp owns aligned groups of 32 vertices = one mask word.
+    for (u32 v0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; v0 < p.n; v0 += stride) {
+        const u32 word = ld_cg(mask_in + (v0 >> 5));
+        if (word == 0u) continue;  // warp-uniform
+        __syncwarp();
+        if (lane == 0) mask_in[v0 >> 5] = 0u;
+        const u32 u = v0 + lane;
+        if (!((word >> lane) & 1u) || u >= p.n) continue;
+        const u32 du = st_dist(ld_state(p.state + u));
+        if (du == INF32) continue;
+        u32 ub = INF32;
+        if constexpr (ASTAR) {
+            ub = st_dist(ld_state(p.state + p.target));
+            if ((u64)du + h_of(p, u) >= ub) continue;
+        }
+        const u32 r0 = __ldg(p.prow + u), r1 = __ldg(p.prow + u + 1);
+        for (u32 e = r0; e < r1; ++e) {
+            const uint2 a = __ldg(p.adj + e);
+            if (a.y == PAD_W) break;  // padding is at the end of the row
+            L.edges++;
+            const u64 nd = (u64)du + a.y;
+            if (nd >= INF32) continue;
+            if constexpr (ASTAR) {
+                if (nd + h_of(p, a.x) >= ub) continue;
+            }
+            if (relax_state<AM>(p.state + a.x, (u32)nd, u, L.atomics)) {
+                L.updates++;
+                atomicOr(mask_out + (a.x >> 5), 1u << (a.x & 31u));
+                if (vload(&c->changed) == 0u) c->changed = 1u;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Compaction round (Compaction::PrefixScan): vertices flagged in the previous
+// round (near_stamp == flag_epoch) are written contiguously into the near
+// queue: block-wide exclusive scan of the flags, one atomicAdd per CTA chunk
+// for its base. No per-push atomics.
+// ---------------------------------------------------------------------------
+__device__ void round_compact(const RunParams& p, const Snap& s, Coop& cs) {
+    Ctl* c = p.ctl;
+    const u32 BS = blockDim.x;
+    const u32 out = s.in_buf ^ 1u;
+    __shared__ u32 s_base;
+    for (u32 base = blockIdx.x * BS; base < p.total; base += gridDim.x * BS) {
+        const u32 i = base + threadIdx.x;
+        const u32 f = (i < p.total && ld_cg(p.near_stamp + i) == s.flag_epoch) ? 1u : 0u;
+        u32 total = 0;
+        const u32 off = block_exclusive_scan(f, cs.wsum, total);
+        if (total == 0) continue;  // block-uniform
+        if (threadIdx.x == 0) s_base = atomicAdd(&c->cnt[C_NEAR0 + out], total);
+        __syncthreads();
+        if (f) p.nearq[out][s_base + off] = i;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Learned Delta policy: 12 features -> 3 x 64 ReLU -> 8 logits; the argmax
+// picks a multiple of the automatic Delta. Evaluated by the CTA that runs a
+// bucket-advance transition.
+// ---------------------------------------------------------------------------
+__device__ u32 policy_pick(const PolicyNet* net, const float* feat, float* act0, float* act1) {
+    const u32 t = threadIdx.x;
+    __shared__ float s_in[POL_IN];
+    __shared__ float s_logit[POL_OUT];
+    if (t < POL_IN) s_in[t] = (feat[t] - net->in_mean[t]) * net->in_scale[t];
+    __syncthreads();
+    if (t < POL_H) {
+        float a = net->b1[t];
+        for (int i = 0; i < POL_IN; ++i) a = fmaf(net->w1[t * POL_IN + i], s_in[i], a);
+        act0[t] = a > 0.f ? a : 0.f;
+    }
+    __syncthreads();
+    if (t < POL_H) {
+        float a = net->b2[t];
+        for (int i = 0; i < POL_H; ++i) a = fmaf(net->w2[t * POL_H + i], act0[i], a);
+        act1[t] = a > 0.f ? a : 0.f;
+    }
+    __syncthreads();
+    if (t < POL_H) {
+        float a = net->b3[t];
+        for (int i = 0; i < POL_H; ++i) a = fmaf(net->w3[t * POL_H + i], act1[i], a);
+        act0[t] = a > 0.f ? a : 0.f;
+    }
+    __syncthreads();
+    if (t < POL_OUT) {
+        float a = net->b4[t];
+        for (int i = 0; i < POL_H; ++i) a = fmaf(net->w4[t * POL_H + i], act0[i], a);
+        s_logit[t] = a;
+    }
+    __syncthreads();
+    u32 best = 0;
+    for (u32 i = 1; i < (u32)POL_OUT; ++i)
+        if (s_logit[i] > s_logit[best]) best = i;
+    return best;
+}
+
+// ---------------------------------------------------------------------------
+// Transition, run by the CTA that arrives last at a barrier (block-uniform
+// control flow; thread 0 owns the control block, the whole CTA evaluates the
+// policy network when a bucket advance asks for it).
+// ---------------------------------------------------------------------------
+__device__ void transition(const RunParams& p, u32* s_flag, float* s_feat, float* act0,
+                           float* act1) {
+    Ctl* c = p.ctl;
+    volatile Ctl* vc = c;
+    const u32 t = threadIdx.x;
+    // s_flag[0]: 0 = no bucket advance, 1 = advance with the policy, 2 = fixed Delta
+    if (t == 0) {
+        s_flag[0] = 0;
+        const u32 ph = vc->phase;
+        const u32 rounds = vc->rounds;
+        const u32 old_near_epoch = vc->near_epoch;
+        const u32 in_buf = vc->in_buf;
+        const u32 out = in_buf ^ 1u;
+        c->rounds = rounds + 1u;
+        c->near_epoch = old_near_epoch + 1u;  // every round pushes with a fresh stamp
+        c->bucket_rounds = vc->bucket_rounds + 1u;
+        bool advance = false;
+        if (vc->status != DS_OK) {
+            c->phase = PH_DONE;
+        } else if (rounds > vc->round_cap) {
+            c->status = DS_NOT_CONVERGED;
+            c->phase = PH_DONE;
+        } else if (ph == PH_INIT) {
+            // Seed the k sources (reference seedKernel, src/gpu_kernels.cuh:340-352).
+            bool bad = false;
+            for (u32 i = 0; i < p.k; ++i) bad = bad || p.srcs[i] >= p.n;
+            for (u32 i = 0; i < p.k && !bad; ++i) {
+                const u32 gi = i * p.n + p.srcs[i];
+                p.state[gi] = pack_state(0u, NO_PARENT);
+                if (p.mode != MODE_NAIVE) p.nearq[0][i] = gi;
+            }
+            c->iterations = vc->iterations + 1u;
+            if (bad) {
+                c->status = DS_BAD_SOURCE;  // sources given in device memory are checked here
+                c->phase = PH_DONE;
+            } else if (p.mode == MODE_NAIVE) {
+                const u32 src = p.srcs[0];
+                atomicOr(p.naive_mask[0] + (src >> 5), 1u << (src & 31u));
+                c->naive_in = 0u;
+                c->changed = 0u;
+                c->in_count = p.n;
+                c->phase = PH_NAIVE;
+            } else {
+                u64 key0 = 0;
+                if (p.astar && p.use_h)
+                    key0 = heuristic_value(p.x[p.srcs[0]], p.y[p.srcs[0]], p.xt, p.yt, p.hscale);
+                const u64 d = vc->delta;
+                c->cnt[C_NEAR0] = p.k;
+                c->cnt[C_NEAR1] = 0u;
+                c->in_buf = 0u;
+                c->in_count = p.k;
+                c->lo = 0ull;
+                c->hi = p.mode == MODE_FRONTIER ? ~0ull : (key0 / d + 1ull) * d;
+                c->bucket_near = p.k;
+                c->bucket_rounds = 0u;
+                c->phase = PH_LIGHT;
+            }
+        } else if (ph == PH_NAIVE) {
+            c->iterations = vc->iterations + 1u;
+            if (vc->changed == 0u) {
+                c->phase = PH_DONE;
+            } else {
+                c->changed = 0u;
+                c->naive_in = vc->naive_in ^ 1u;
+            }
+        } else if (ph == PH_COMPACT) {
+            const u32 nn = vc->cnt[C_NEAR0 + out];
+            if (nn) {
+                c->cnt[C_NEAR0 + in_buf] = 0u;
+                c->in_buf = out;
+                c->in_count = nn;
+                c->iterations = vc->iterations + 1u;
+                c->phase = PH_LIGHT;
+            } else {
+                c->phase = PH_DONE;
+            }
+        } else if (ph == PH_LIGHT || ph == PH_SCAN) {
+            const u32 nn = vc->cnt[C_NEAR0 + out];
+            if (p.prefix_scan) {
+                // the round just ended flagged its improved vertices with its stamp
+                c->flag_epoch = old_near_epoch;
+                c->cnt[C_NEAR0 + out] = 0u;
+                c->in_count = p.total;
+                c->phase = PH_COMPACT;
+            } else if (nn) {
+                c->cnt[C_NEAR0 + in_buf] = 0u;
+                c->in_buf = out;
+                c->in_count = nn;
+                c->iterations = vc->iterations + 1u;
+                c->bucket_near = vc->bucket_near + nn;
+                c->phase = PH_LIGHT;
+            } else if (vc->heavy && vc->cnt[C_R]) {
+                c->in_count = vc->cnt[C_R];
+                c->iterations = vc->iterations + 1u;
+                c->phase = PH_HEAVY;
+            } else {
+                advance = true;
+            }
+        } else if (ph == PH_HEAVY) {
+            c->cnt[C_R] = 0u;
+            c->r_epoch = vc->r_epoch + 1u;  // R may be refilled in this bucket (A*)
+            const u32 nn = vc->cnt[C_NEAR0 + out];
+            if (nn) {
+                c->cnt[C_NEAR0 + in_buf] = 0u;
+                c->in_buf = out;
+                c->in_count = nn;
+                c->iterations = vc->iterations + 1u;
+                c->phase = PH_LIGHT;
+            } else {
+                advance = true;
+            }
+        }
+        if (advance) {
+            c->buckets = vc->buckets + 1u;
+            const u32 fin = vc->far_out;
+            const u32 fn = vc->cnt[C_FAR0 + fin];
+            const u64 est = vc->far_min[fin];
+            if (fn == 0u || est == ~0ull) {
+                c->phase = PH_DONE;
+            } else {
+                s_flag[0] = p.policy ? 1u : 2u;
+                if (p.policy) {
+                    const double aw = p.avg_w > 0.0 ? p.avg_w : 1.0;
+                    const u64 edges_now = vc->bucket_edges_acc;
+                    s_feat[0] = log2f(1.f + (float)fn);
+                    s_feat[1] = log2f(1.f + (float)vc->bucket_near);
+                    s_feat[2] = log2f(1.f + (float)vc->bucket_rounds);
+                    s_feat[3] = (float)((double)(est - vc->hi) / aw);
+                    s_feat[4] = log2f(1.f + (float)(edges_now - vc->bucket_edges));
+                    s_feat[5] = log2f(1.f + (float)vc->buckets);
+                    s_feat[6] = log2f((float)((double)vc->delta / aw));
+                    s_feat[7] = log2f(1.f + (float)p.avg_deg);
+                    s_feat[8] = log2f((float)((double)p.maxw / aw));
+                    s_feat[9] = log2f(1.f + (float)p.n);
+                    s_feat[10] = (float)((double)est / (aw * sqrt((double)p.n)));
+                    s_feat[11] = fminf(1.f, (float)vc->delta / (float)(p.maxw ? p.maxw : 1u));
+                    c->bucket_edges = edges_now;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const u32 need = s_flag[0];
+    if (need == 1u) {
+        const u32 cls = policy_pick(p.net, s_feat, act0, act1);
+        if (t == 0) s_flag[1] = cls;
+    }
+    __syncthreads();
+    if (t == 0 && need != 0u) {
+        // Open the next bucket: the far pile collected during this bucket is
+        // scanned against the window [old hi, new hi).
+        u32 d = p.delta;
+        if (need == 1u) {
+            const float dm = (float)p.delta * kPolicyMult[s_flag[1]];
+            d = dm < 1.f ? 1u : (dm > 2.0e9f ? 2000000000u : (u32)dm);
+            c->policy_calls = vc->policy_calls + 1u;
+        }
+        const u32 fin = vc->far_out;
+        const u64 est = vc->far_min[fin];
+        c->delta = d;
+        c->heavy = d < p.maxw ? 1u : 0u;
+        c->lo = vc->hi;
+        c->hi = need == 1u ? est + d : (est / d + 1ull) * d;
+        c->far_in = fin;
+        c->far_out = fin ^ 1u;
+        c->cnt[C_FAR0 + (fin ^ 1u)] = 0u;
+        c->far_min[fin ^ 1u] = ~0ull;
+        c->far_epoch = vc->far_epoch + 1u;
+        c->r_epoch = vc->r_epoch + 1u;
+        c->in_count = vc->cnt[C_FAR0 + fin];
+        c->iterations = vc->iterations + 1u;
+        c->bucket_near = 0u;
+        c->bucket_rounds = 0u;
+        c->phase = PH_SCAN;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Bounded grid barrier. The last CTA to arrive runs `transition`, then opens
+// the barrier. A CTA that waits longer than p.timeout_ns, or sees an error
+// status, stops waiting and the kernel winds down; no wait is unbounded.
+// ---------------------------------------------------------------------------
+__device__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, u32* s_flag,
+                             float* s_feat, float* act0, float* act1) {
+    __syncthreads();
+    Ctl* c = p.ctl;
+    const u64 fmin = block_min_u64(L.fmin, red);
+    L.fmin = ~0ull;
+    __shared__ u32 s_last, s_gen;
+    if (threadIdx.x == 0) {
+        if (fmin != ~0ull) atomicMin((unsigned long long*)&c->far_min[s.far_out], (unsigned long long)fmin);
+        const u32 gen = vload(&c->bar_gen);
+        __threadfence();
+        const u32 arrived = atomicAdd(&c->bar_count, 1u) + 1u;
+        s_gen = gen;
+        s_last = arrived == gridDim.x ? 1u : 0u;
+    }
+    __syncthreads();
+    if (s_last) {
+        if (threadIdx.x == 0) {
+            c->bar_count = 0;
+            __threadfence();
+        }
+        transition(p, s_flag, s_feat, act0, act1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicExch(&c->bar_gen, s_gen + 1u);
+        }
+    } else if (threadIdx.x == 0) {
+        const u64 t0 = global_timer_ns();
+        u32 spins = 0;
+        while (vload(&c->bar_gen) == s_gen) {
+            __nanosleep(32);
+            if ((++spins & 63u) == 0u) {
+                if (vload(&c->status) != DS_OK) break;
+                if (global_timer_ns() - t0 > p.timeout_ns) {
+                    atomicCAS(&c->status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                    break;
+                }
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s.phase = vload(&c->phase);
+        s.in_count = vload(&c->in_count);
+        s.in_buf = vload(&c->in_buf);
+        s.far_in = vload(&c->far_in);
+        s.far_out = vload(&c->far_out);
+        s.status = vload(&c->status);
+        s.delta = vload(&c->delta);
+        s.heavy = vload(&c->heavy);
+        s.near_epoch = vload(&c->near_epoch);
+        s.far_epoch = vload(&c->far_epoch);
+        s.r_epoch = vload(&c->r_epoch);
+        s.naive_in = vload(&c->naive_in);
+        s.flag_epoch = vload(&c->flag_epoch);
+        s.map_mode = 1u;
+        s.lo = vload64(&c->lo);
+        s.hi = vload64(&c->hi);
+        if (s.status != DS_OK) s.phase = PH_DONE;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// The persistent kernel.
+// ---------------------------------------------------------------------------
+template <bool ASTAR, int AM, int MAP>
+__global__ void __launch_bounds__(MAX_BS) k_persistent(const __grid_constant__ RunParams p) {
+    __shared__ Snap s;
+    __shared__ Coop cs;
+    __shared__ u64 red[32];
+    __shared__ u32 s_flag[2];
+    __shared__ float s_feat[POL_IN];
+    __shared__ float act0[POL_H], act1[POL_H];
+    Local L;
+
+    // INIT: every state word to (INF, NO_PARENT) (reference initStateKernel,
+    // src/gpu_kernels.cuh:334-337).
+    const u64 gtid = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 gstride = (u64)gridDim.x * blockDim.x;
+    for (u64 i = gtid; i < p.total; i += gstride) p.state[i] = STATE_INIT;
+    if (threadIdx.x == 0) s.far_out = 0;
+    grid_barrier(p, s, L, red, s_flag, s_feat, act0, act1);
+
+    while (s.phase != PH_DONE) {
+        const u32 ph = s.phase;
+        if (ph == PH_LIGHT) {
+            round_items<ASTAR, AM, MAP>(p, s, p.nearq[s.in_buf], s.in_count, K_LIGHT, L, cs);
+        } else if (ph == PH_SCAN) {
+            round_items<ASTAR, AM, MAP>(p, s, p.farq[s.far_in], s.in_count, K_SCAN, L, cs);
+        } else if (ph == PH_HEAVY) {
+            round_items<ASTAR, AM, MAP>(p, s, p.rq, s.in_count, K_HEAVY, L, cs);
+        } else if (ph == PH_NAIVE) {
+            round_naive<ASTAR, AM>(p, s, L);
+        } else if (ph == PH_COMPACT) {
+            round_compact(p, s, cs);
+        }
+        grid_barrier(p, s, L, red, s_flag, s_feat, act0, act1);
+    }
+
+    // Per-warp reduction of the counters, one atomicAdd per warp.
+    unsigned long long a = L.edges, b = L.atomics, cc = L.updates, d = L.pushes;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(FULL, a, o);
+        b += __shfl_down_sync(FULL, b, o);
+        cc += __shfl_down_sync(FULL, cc, o);
+        d += __shfl_down_sync(FULL, d, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        unsigned long long* st = p.ctl->stats;
+        if (a) atomicAdd(&st[0], a);
+        if (b) atomicAdd(&st[1], b);
+        if (cc) atomicAdd(&st[2], cc);
+        if (d) atomicAdd(&st[3], d);
+    }
+}
+
+}  // namespace pfg
+
+// ===========================================================================
+// Host-side launch helpers
+// ===========================================================================
+namespace pfg {
+
+typedef void (*KernelFn)(RunParams);
+
+template <bool A>
+static KernelFn pick_am_map(int am, int map) {
+    switch (am * 3 + map) {
+        case 0: return k_persistent<A, 0, 0>;
+        case 1: return k_persistent<A, 0, 1>;
+        case 2: return k_persistent<A, 0, 2>;
+        case 3: return k_persistent<A, 1, 0>;
+        case 4: return k_persistent<A, 1, 1>;
+        case 5: return k_persistent<A, 1, 2>;
+        case 6: return k_persistent<A, 2, 0>;
+        case 7: return k_persistent<A, 2, 1>;
+        default: return k_persistent<A, 2, 2>;
+    }
+}
+
+static const void* kernel_for(bool astar, int am, int map) {
+    if (am < 0 || am > 2) am = 0;
+    if (map < 0 || map > 2) map = 2;
+    return astar ? (const void*)pick_am_map<true>(am, map) : (const void*)pick_am_map<false>(am, map);
+}
+
+cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, int block,
+                              int grid, cudaStream_t st) {
+    void* args[] = {(void*)&p};
+    return cudaLaunchCooperativeKernel(kernel_for(astar, am, map), dim3(grid), dim3(block), args,
+                                       0, st);
+}
+
+int persistent_blocks_per_sm(bool astar, int am, int map, int block) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel_for(astar, am, map), block, 0) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return nb;
+}
+
+// One warp per vertex copies its row into the padded slot.
+__global__ void k_build_adj(const u32* __restrict__ row, const u32* __restrict__ col,
+                            const u32* __restrict__ w, const u32* __restrict__ prow, u32 n,
+                            uint2* __restrict__ adj) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 u = warp; u < n; u += nwarps) {
+        const u32 r0 = row[u], deg = row[u + 1] - r0;
+        const u32 p0 = prow[u], pd = prow[u + 1] - p0;
+        for (u32 j = lane; j < pd; j += 32)
+            adj[p0 + j] = j < deg ? make_uint2(col[r0 + j], w[r0 + j]) : make_uint2(u, PAD_W);
+    }
+}
+
+cudaError_t launch_build_adj(const uint32_t* row, const uint32_t* col, const uint32_t* w,
+                             const uint32_t* prow, uint32_t n, void* adj, cudaStream_t st) {
+    const int bs = 256;
+    u32 blocks = (u32)((n + 7u) / 8u);
+    if (blocks > 65535u * 4u) blocks = 65535u * 4u;
+    if (blocks == 0) blocks = 1;
+    k_build_adj<<<blocks, bs, 0, st>>>(row, col, w, prow, n, (uint2*)adj);
+    return cudaGetLastError();
+}
+
+// Single-thread walk of the parent chain (reference reconstructPath,
+// src/cpu_sssp.cpp:124-135): at most n+1 steps, so it always terminates.
+__global__ void k_extract_path(const u64* __restrict__ state, u64 base, u32 n, u32 src, u32 dst,
+                               u32* __restrict__ path_rev, u32 cap, u32* __restrict__ len) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    u32 v = dst, count = 0;
+    for (u64 steps = 0; steps <= n; ++steps) {
+        if (count < cap) path_rev[count] = v;
+        ++count;
+        if (v == src) {
+            *len = count <= cap ? count : cap + 1u;
+            return;
+        }
+        const u32 pv = (u32)(__ldcg(state + base + v) & 0xFFFFFFFFull);
+        if (pv == NO_PARENT || pv >= n) break;
+        v = pv;
+    }
+    *len = 0;  // broken chain, cycle, or unreachable
+}
+
+cudaError_t launch_extract_path(const uint64_t* state, uint64_t base, uint32_t n, uint32_t src,
+                                uint32_t dst, uint32_t* path_rev, uint32_t cap, uint32_t* len,
+                                cudaStream_t st) {
+    k_extract_path<<<1, 32, 0, st>>>(state, base, n, src, dst, path_rev, cap, len);
+    return cudaGetLastError();
+}
+
+}  // namespace pfg

@@ -1,0 +1,655 @@
+// pfg_solver.cu - host orchestration and C ABI of the B200 SSSP / A* engine.
+//
+// Replaces the reference's GpuSolver::Impl (src/gpu_sssp.cu:61-534): one-time
+// device allocation and CSR upload, then one persistent cooperative launch per
+// query. Errors are reported as pfg_status codes plus a thread-local message
+// instead of exit() (reference: src/cuda_check.cuh:9-17) and exceptions.
+#include "../../include/pfg.h"
+#include "pfg_common.cuh"
+#include "pfg_kernels.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace pfg;
+
+// ---------------------------------------------------------------------------
+// Error handling
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static pfg_status fail(pfg_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+#define PFG_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e__ = (call);                                                        \
+        if (e__ != cudaSuccess) {                                                        \
+            const pfg_status st__ = e__ == cudaErrorMemoryAllocation ? PFG_ERR_OUT_OF_MEMORY \
+                                                                     : PFG_ERR_CUDA;     \
+            cudaGetLastError();                                                          \
+            return fail(st__, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e__),   \
+                        __FILE__, __LINE__);                                             \
+        }                                                                                \
+    } while (0)
+
+extern "C" const char* pfg_last_error(void) { return g_last_error.c_str(); }
+extern "C" void pfg_internal_set_error(const char* msg) { g_last_error = msg ? msg : ""; }
+extern "C" int32_t pfg_abi_version(void) { return PFG_ABI_VERSION; }
+extern "C" const char* pfg_status_string(pfg_status st) {
+    switch (st) {
+        case PFG_OK: return "ok";
+        case PFG_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case PFG_ERR_INVALID_GRAPH: return "invalid graph";
+        case PFG_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case PFG_ERR_NOT_CONVERGED: return "did not converge";
+        case PFG_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+        case PFG_ERR_CUDA: return "CUDA error";
+        case PFG_ERR_NO_DEVICE: return "no CUDA device";
+        case PFG_ERR_CAPACITY: return "capacity exceeded";
+    }
+    return "unknown status";
+}
+
+// ---------------------------------------------------------------------------
+// Solver object
+// ---------------------------------------------------------------------------
+struct pfg_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    u32 n = 0, m = 0, K = 1, maxw = 0;
+    u64 m_pad = 0;
+    double hscale = 0.0, avg_w = 0.0, avg_deg = 0.0;
+    bool has_xy = false;
+    std::vector<double> hx, hy;  // host copies of the coordinates (A* target lookup)
+    int sm_count = 1;
+    double upload_ms = 0.0;
+    u64 bytes = 0;
+
+    uint2* d_adj = nullptr;
+    u32* d_prow = nullptr;
+    double* d_x = nullptr;
+    double* d_y = nullptr;
+    u64* d_state = nullptr;
+    u32* d_q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // near0, near1, far0, far1, R
+    u32* d_stamp[3] = {nullptr, nullptr, nullptr};                // near, far, R
+    u32* d_naive[2] = {nullptr, nullptr};
+    u32* d_srcs = nullptr;
+    u32* d_path = nullptr;      // path extraction scratch [n + 1]
+    u32* d_path_len = nullptr;
+    Ctl* d_ctl = nullptr;
+    PolicyNet* d_net = nullptr;
+    bool has_net = false;
+
+    Ctl* h_ctl = nullptr;       // pinned mirror of the control block
+    u32* h_srcs = nullptr;      // pinned staging of the sources [K]
+
+    // last asynchronous run
+    bool pending = false;
+    pfg_status pending_status = PFG_OK;
+    int last_mode = MODE_DELTA;
+    u32 last_delta = 0;
+    u32 last_k = 0;
+    u32 epoch_hint = 1;   // largest epoch known to the host (stamps reset near 2^32)
+    std::vector<void*> allocs;
+
+    template <class T>
+    pfg_status dalloc(T** p, u64 count) {
+        void* q = nullptr;
+        const u64 b = std::max<u64>(1, count) * sizeof(T);
+        cudaError_t e = cudaMalloc(&q, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(PFG_ERR_OUT_OF_MEMORY, "cudaMalloc of %.1f MB failed: %s", b / 1048576.0,
+                        cudaGetErrorString(e));
+        }
+        allocs.push_back(q);
+        bytes += b;
+        *p = (T*)q;
+        return PFG_OK;
+    }
+};
+
+static u32 auto_delta_of(double avg_w, double avg_deg) {
+    // Davidson et al.: Delta ~ warp size * average weight / average degree
+    // (reference: src/gpu_sssp.cu:202-206).
+    const double d = 32.0 * avg_w / std::max(1.0, avg_deg);
+    const long long r = std::llround(d);
+    return (u32)std::max<long long>(1, std::min<long long>(r, 0x7FFFFFFFll));
+}
+
+static void destroy_solver(pfg_solver* s) {
+    if (!s) return;
+    if (s->device >= 0) cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->h_ctl) cudaFreeHost(s->h_ctl);
+    if (s->h_srcs) cudaFreeHost(s->h_srcs);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    cudaGetLastError();
+    delete s;
+}
+
+static pfg_status validate_csr(const uint32_t* row, const uint32_t* col, const uint32_t* w,
+                               uint32_t n, uint32_t m, u32* maxw_out) {
+    if (n == 0) return fail(PFG_ERR_INVALID_GRAPH, "graph has no vertices");
+    if (!row || (m > 0 && (!col || !w)))
+        return fail(PFG_ERR_INVALID_GRAPH, "CSR arrays must not be NULL");
+    if (row[0] != 0) return fail(PFG_ERR_INVALID_GRAPH, "row_offsets[0] must be 0");
+    if (row[n] != m) return fail(PFG_ERR_INVALID_GRAPH, "row_offsets[n] = %u but m = %u", row[n], m);
+    u32 maxw = 0;
+    for (u32 u = 0; u < n; ++u) {
+        const u32 b = row[u], e = row[u + 1];
+        if (e < b) return fail(PFG_ERR_INVALID_GRAPH, "row_offsets decreases at vertex %u", u);
+        for (u32 k = b; k < e; ++k) {
+            if (col[k] >= n) return fail(PFG_ERR_INVALID_GRAPH, "col_indices[%u] = %u >= n", k, col[k]);
+            if (w[k] == 0 || w[k] == PAD_W)
+                return fail(PFG_ERR_INVALID_GRAPH, "weights[%u] = %u outside [1, 2^32-2]", k, w[k]);
+            if (k > b && w[k] < w[k - 1])
+                return fail(PFG_ERR_INVALID_GRAPH,
+                            "row %u is not sorted by weight (arc %u); build the CSR with rows "
+                            "sorted by (w, dst)", u, k);
+            maxw = std::max(maxw, w[k]);
+        }
+    }
+    *maxw_out = maxw;
+    return PFG_OK;
+}
+
+extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* col,
+                                           const uint32_t* w, const double* x, const double* y,
+                                           uint32_t n, uint32_t m, double h_scale, double avg_w,
+                                           double avg_deg, uint32_t max_batch, int32_t device,
+                                           pfg_solver** out) {
+    if (!out) return fail(PFG_ERR_INVALID_ARGUMENT, "out must not be NULL");
+    *out = nullptr;
+    if ((x == nullptr) != (y == nullptr))
+        return fail(PFG_ERR_INVALID_ARGUMENT, "x and y must both be set or both be NULL");
+    u32 maxw = 0;
+    pfg_status st = validate_csr(row, col, w, n, m, &maxw);
+    if (st != PFG_OK) return st;
+    const u32 K = std::max<u32>(1, max_batch);
+    if ((u64)K * n >= 0xFFFFFFFFull)
+        return fail(PFG_ERR_INVALID_ARGUMENT, "maxBatch * n must be < 2^32");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) {
+        cudaGetLastError();
+        return fail(PFG_ERR_NO_DEVICE, "CUDA device %d not available", device);
+    }
+
+    // Padded row starts: each row rounded up to a multiple of 4 arcs.
+    std::vector<u32> prow((size_t)n + 1);
+    u64 acc = 0;
+    for (u32 u = 0; u < n; ++u) {
+        prow[u] = (u32)acc;
+        const u32 deg = row[u + 1] - row[u];
+        acc += (u64)((deg + ROW_ALIGN - 1) / ROW_ALIGN) * ROW_ALIGN;
+        if (acc >= 0xFFFFFFF0ull) return fail(PFG_ERR_INVALID_GRAPH, "padded arc count exceeds 2^32");
+    }
+    prow[n] = (u32)acc;
+
+    pfg_solver* s = new pfg_solver();
+    s->device = device;
+    s->n = n;
+    s->m = m;
+    s->K = K;
+    s->maxw = maxw;
+    s->m_pad = acc;
+    s->hscale = h_scale;
+    s->avg_w = avg_w;
+    s->avg_deg = avg_deg;
+    s->has_xy = x != nullptr;
+    auto bail = [&](pfg_status e) {
+        destroy_solver(s);
+        return e;
+    };
+#define TRY(expr)                                   \
+    do {                                            \
+        pfg_status e_ = (expr);                     \
+        if (e_ != PFG_OK) return bail(e_);          \
+    } while (0)
+#define TRYC(call)                                                                          \
+    do {                                                                                    \
+        cudaError_t e__ = (call);                                                           \
+        if (e__ != cudaSuccess) {                                                           \
+            cudaGetLastError();                                                             \
+            return bail(fail(e__ == cudaErrorMemoryAllocation ? PFG_ERR_OUT_OF_MEMORY       \
+                                                              : PFG_ERR_CUDA,               \
+                             "%s failed: %s", #call, cudaGetErrorString(e__)));            \
+        }                                                                                   \
+    } while (0)
+
+    TRYC(cudaSetDevice(device));
+    TRYC(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device));
+    int coop = 0;
+    TRYC(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    if (!coop) return bail(fail(PFG_ERR_NO_DEVICE, "device %d lacks cooperative launch", device));
+
+    // Memory precheck (reference: src/gpu_sssp.cu:113-127).
+    const u64 Kn = (u64)K * n;
+    const u64 need = s->m_pad * 8 + (u64)(n + 1) * 4 + (s->has_xy ? (u64)n * 16 : 0) + Kn * 8 +
+                     5 * Kn * 4 + 3 * Kn * 4 + 2 * ((u64)n / 32 + 1) * 4 + (u64)(n + 1) * 4 +
+                     ((u64)n + 1) * 4 + 2 * (u64)m * 4;  // last term: upload staging on device
+    size_t free_b = 0, total_b = 0;
+    TRYC(cudaMemGetInfo(&free_b, &total_b));
+    if (need > free_b)
+        return bail(fail(PFG_ERR_OUT_OF_MEMORY,
+                         "Not enough GPU memory: need %.1f MB, free %.1f MB (reduce graph or batch)",
+                         need / 1048576.0, free_b / 1048576.0));
+
+    TRYC(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    TRYC(cudaEventCreate(&s->ev0));
+    TRYC(cudaEventCreate(&s->ev1));
+
+    // ---- upload: pinned staging, three streams (reference: src/gpu_sssp.cu:138-152),
+    //      then the padded adjacency is built on the device ----
+    auto t0 = std::chrono::steady_clock::now();
+    TRY(s->dalloc(&s->d_adj, s->m_pad));
+    TRY(s->dalloc(&s->d_prow, (u64)n + 1));
+    {
+        u32 *d_row = nullptr, *d_col = nullptr, *d_w = nullptr;
+        TRYC(cudaMalloc((void**)&d_row, ((size_t)n + 1) * 4));
+        TRYC(cudaMalloc((void**)&d_col, std::max<size_t>(1, (size_t)m) * 4));
+        TRYC(cudaMalloc((void**)&d_w, std::max<size_t>(1, (size_t)m) * 4));
+        const size_t bRow = ((size_t)n + 1) * 4, bCol = (size_t)m * 4, bW = (size_t)m * 4;
+        char* stage = nullptr;
+        cudaError_t e = cudaMallocHost((void**)&stage, 2 * bRow + bCol + bW);
+        if (e != cudaSuccess) {
+            cudaFree(d_row); cudaFree(d_col); cudaFree(d_w);
+            cudaGetLastError();
+            return bail(fail(PFG_ERR_OUT_OF_MEMORY, "pinned staging allocation failed"));
+        }
+        memcpy(stage, row, bRow);
+        memcpy(stage + bRow, prow.data(), bRow);
+        if (m) {
+            memcpy(stage + 2 * bRow, col, bCol);
+            memcpy(stage + 2 * bRow + bCol, w, bW);
+        }
+        cudaStream_t st[3];
+        bool ok = true;
+        for (auto& q : st) ok = ok && cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) == cudaSuccess;
+        if (ok) {
+            ok = cudaMemcpyAsync(d_row, stage, bRow, cudaMemcpyHostToDevice, st[0]) == cudaSuccess &&
+                 cudaMemcpyAsync(s->d_prow, stage + bRow, bRow, cudaMemcpyHostToDevice, st[0]) == cudaSuccess &&
+                 (m == 0 || cudaMemcpyAsync(d_col, stage + 2 * bRow, bCol, cudaMemcpyHostToDevice, st[1]) == cudaSuccess) &&
+                 (m == 0 || cudaMemcpyAsync(d_w, stage + 2 * bRow + bCol, bW, cudaMemcpyHostToDevice, st[2]) == cudaSuccess);
+            for (auto& q : st) {
+                ok = cudaStreamSynchronize(q) == cudaSuccess && ok;
+                cudaStreamDestroy(q);
+            }
+        }
+        if (ok) ok = launch_build_adj(d_row, d_col, d_w, s->d_prow, n, s->d_adj, s->stream) == cudaSuccess;
+        if (ok) ok = cudaStreamSynchronize(s->stream) == cudaSuccess;
+        cudaFreeHost(stage);
+        cudaFree(d_row);
+        cudaFree(d_col);
+        cudaFree(d_w);
+        if (!ok) {
+            cudaError_t le = cudaGetLastError();
+            return bail(fail(PFG_ERR_CUDA, "CSR upload failed: %s", cudaGetErrorString(le)));
+        }
+    }
+    if (s->has_xy) {
+        TRY(s->dalloc(&s->d_x, n));
+        TRY(s->dalloc(&s->d_y, n));
+        TRYC(cudaMemcpy(s->d_x, x, (size_t)n * 8, cudaMemcpyHostToDevice));
+        TRYC(cudaMemcpy(s->d_y, y, (size_t)n * 8, cudaMemcpyHostToDevice));
+        s->hx.assign(x, x + n);
+        s->hy.assign(y, y + n);
+    }
+    s->upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+
+    // ---- working set, allocated once (reference: src/gpu_sssp.cu:160-186) ----
+    TRY(s->dalloc(&s->d_state, Kn));
+    for (int i = 0; i < 5; ++i) TRY(s->dalloc(&s->d_q[i], Kn));
+    for (int i = 0; i < 3; ++i) {
+        TRY(s->dalloc(&s->d_stamp[i], Kn));
+        TRYC(cudaMemsetAsync(s->d_stamp[i], 0, Kn * 4, s->stream));
+    }
+    const u64 words = (u64)n / 32 + 1;
+    for (int i = 0; i < 2; ++i) {
+        TRY(s->dalloc(&s->d_naive[i], words));
+        TRYC(cudaMemsetAsync(s->d_naive[i], 0, words * 4, s->stream));
+    }
+    TRY(s->dalloc(&s->d_srcs, K));
+    TRY(s->dalloc(&s->d_path, (u64)n + 1));
+    TRY(s->dalloc(&s->d_path_len, 1));
+    TRY(s->dalloc(&s->d_ctl, 1));
+    TRY(s->dalloc(&s->d_net, 1));
+    TRYC(cudaMallocHost((void**)&s->h_ctl, sizeof(Ctl)));
+    TRYC(cudaMallocHost((void**)&s->h_srcs, (size_t)K * 4));
+    memset(s->h_ctl, 0, sizeof(Ctl));
+    s->h_ctl->near_epoch = 1;
+    s->h_ctl->far_epoch = 1;
+    s->h_ctl->r_epoch = 1;
+    TRYC(cudaMemcpyAsync(s->d_ctl, s->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, s->stream));
+    TRYC(cudaStreamSynchronize(s->stream));
+    *out = s;
+    return PFG_OK;
+#undef TRY
+#undef TRYC
+}
+
+extern "C" pfg_status pfg_create(const uint32_t* row, const uint32_t* col, const uint32_t* w,
+                                 const double* x, const double* y, uint32_t n, uint32_t m,
+                                 double h_scale, double avg_w, double avg_deg, uint32_t max_batch,
+                                 pfg_solver** out) {
+    return pfg_create_on_device(row, col, w, x, y, n, m, h_scale, avg_w, avg_deg, max_batch, 0, out);
+}
+
+extern "C" void pfg_destroy(pfg_solver* s) { destroy_solver(s); }
+extern "C" double pfg_upload_ms(const pfg_solver* s) { return s ? s->upload_ms : 0.0; }
+extern "C" uint64_t pfg_device_bytes(const pfg_solver* s) { return s ? s->bytes : 0; }
+extern "C" uint32_t pfg_auto_delta(const pfg_solver* s) {
+    return s ? auto_delta_of(s->avg_w, s->avg_deg) : 0u;
+}
+extern "C" uint32_t pfg_num_vertices(const pfg_solver* s) { return s ? s->n : 0u; }
+extern "C" uint32_t pfg_max_batch(const pfg_solver* s) { return s ? s->K : 0u; }
+extern "C" void* pfg_stream(const pfg_solver* s) { return s ? (void*)s->stream : nullptr; }
+extern "C" const uint64_t* pfg_state_device(const pfg_solver* s) { return s ? s->d_state : nullptr; }
+
+// ---------------------------------------------------------------------------
+// Runs
+// ---------------------------------------------------------------------------
+static int env_int(const char* name, int dflt) {
+    const char* v = getenv(name);
+    if (!v || !*v) return dflt;
+    return atoi(v);
+}
+
+static pfg_options default_options() {
+    pfg_options o;
+    o.algo = PFG_ALGO_DELTA;
+    o.mapping = PFG_MAP_HYBRID;
+    o.atomic = PFG_ATOMIC_MIN_RBA;
+    o.delta = 0;
+    o.block_size = 256;
+    o.sync_every = 8;
+    o.compaction = PFG_COMPACT_WARP_ATOMIC;
+    o.policy = PFG_POLICY_FIXED;
+    return o;
+}
+
+// Resets the stamp words when the epoch counters approach 2^32.
+static pfg_status maybe_reset_epochs(pfg_solver* s) {
+    if (s->epoch_hint < 0xF0000000u) return PFG_OK;
+    const u64 Kn = (u64)s->K * s->n;
+    for (int i = 0; i < 3; ++i) PFG_CUDA(cudaMemsetAsync(s->d_stamp[i], 0, Kn * 4, s->stream));
+    Ctl tmp;
+    memset(&tmp, 0, sizeof(tmp));
+    tmp.near_epoch = tmp.far_epoch = tmp.r_epoch = 1;
+    const size_t off = offsetof(Ctl, persist);
+    PFG_CUDA(cudaMemcpyAsync((char*)s->d_ctl + off, (char*)&tmp + off, sizeof(Ctl) - off,
+                             cudaMemcpyHostToDevice, s->stream));
+    PFG_CUDA(cudaStreamSynchronize(s->stream));
+    s->epoch_hint = 1;
+    return PFG_OK;
+}
+
+// Enqueues one run on the solver's stream. h_srcs (host) or d_srcs (device).
+static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint32_t* d_srcs,
+                              uint32_t k, int32_t astar, uint32_t dst, const pfg_options* opt_in,
+                              bool timed) {
+    if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
+    pfg_options o = opt_in ? *opt_in : default_options();
+    // Silent fix-ups of the reference (src/gpu_sssp.cu:462,466).
+    if (o.block_size < 32 || o.block_size > 1024 || (o.block_size % 32) != 0) o.block_size = 256;
+    if (k == 0 || k > s->K) return fail(PFG_ERR_INVALID_ARGUMENT, "invalid batch size");
+    if (h_srcs) {
+        for (u32 i = 0; i < k; ++i)
+            if (h_srcs[i] >= s->n) return fail(PFG_ERR_INVALID_ARGUMENT, "source out of range");
+    } else if (!d_srcs) {
+        return fail(PFG_ERR_INVALID_ARGUMENT, "sources are NULL");
+    }
+    if (astar && dst >= s->n) return fail(PFG_ERR_INVALID_ARGUMENT, "target out of range");
+    if (astar && k != 1) return fail(PFG_ERR_INVALID_ARGUMENT, "A* runs take exactly one source");
+    if (o.algo < 0 || o.algo > 2) return fail(PFG_ERR_INVALID_ARGUMENT, "unknown algorithm %d", o.algo);
+    if (o.algo == PFG_ALGO_NAIVE && k > 1) o.algo = PFG_ALGO_DELTA;
+    if (o.policy == PFG_POLICY_LEARNED && !s->has_net)
+        return fail(PFG_ERR_INVALID_ARGUMENT, "learned policy requested but no network is loaded");
+    PFG_CUDA(cudaSetDevice(s->device));
+    pfg_status st = maybe_reset_epochs(s);
+    if (st != PFG_OK) return st;
+
+    const int mode = o.algo == PFG_ALGO_NAIVE ? MODE_NAIVE
+                   : o.algo == PFG_ALGO_FRONTIER ? MODE_FRONTIER : MODE_DELTA;
+    const u32 delta = mode == MODE_DELTA ? (o.delta ? o.delta : auto_delta_of(s->avg_w, s->avg_deg)) : 0u;
+
+    // Control block for this run (the persistent epoch part is left alone).
+    Ctl* c = s->h_ctl;
+    const size_t run_bytes = offsetof(Ctl, persist);
+    memset(c, 0, run_bytes);
+    c->phase = PH_INIT;
+    c->far_out = 0;
+    c->far_min[0] = c->far_min[1] = ~0ull;
+    const u64 cap = 4ull * s->n + 1000ull;
+    c->round_cap = (u32)std::min<u64>(cap, 0x7FFFFFFFull);
+    c->delta = delta ? delta : 1u;
+    c->delta0 = delta;
+    c->heavy = (mode == MODE_DELTA && delta < s->maxw) ? 1u : 0u;
+
+    RunParams p;
+    memset(&p, 0, sizeof(p));
+    p.adj = s->d_adj;
+    p.prow = s->d_prow;
+    p.x = s->d_x;
+    p.y = s->d_y;
+    p.n = s->n;
+    p.maxw = s->maxw;
+    p.hscale = s->hscale;
+    p.avg_w = s->avg_w;
+    p.avg_deg = s->avg_deg;
+    p.m = s->m;
+    p.k = k;
+    p.total = k * s->n;
+    p.srcs = d_srcs ? d_srcs : s->d_srcs;
+    p.astar = astar ? 1 : 0;
+    p.target = astar ? dst : 0u;
+    p.use_h = (astar && s->has_xy && s->hscale > 0.0) ? 1 : 0;
+    if (p.use_h) {
+        p.xt = s->hx[dst];
+        p.yt = s->hy[dst];
+    }
+    p.state = s->d_state;
+    p.nearq[0] = s->d_q[0];
+    p.nearq[1] = s->d_q[1];
+    p.farq[0] = s->d_q[2];
+    p.farq[1] = s->d_q[3];
+    p.rq = s->d_q[4];
+    p.near_stamp = s->d_stamp[0];
+    p.far_stamp = s->d_stamp[1];
+    p.r_stamp = s->d_stamp[2];
+    p.naive_mask[0] = s->d_naive[0];
+    p.naive_mask[1] = s->d_naive[1];
+    p.ctl = s->d_ctl;
+    p.delta = delta ? delta : 1u;
+    p.mode = mode;
+    p.prefix_scan = (mode == MODE_FRONTIER && o.compaction == PFG_COMPACT_PREFIX_SCAN) ? 1 : 0;
+    p.policy = (mode == MODE_DELTA && o.policy == PFG_POLICY_LEARNED) ? 1 : 0;
+    p.net = s->d_net;
+    p.timeout_ns = (u64)std::max(1, env_int("PFG_TIMEOUT_MS", 2000)) * 1000000ull;
+
+    const int map = mode == MODE_NAIVE ? PFG_MAP_THREAD : o.mapping;
+    const int block = o.block_size;
+    int bps = persistent_blocks_per_sm(astar != 0, o.atomic, map, block);
+    if (bps <= 0) return fail(PFG_ERR_CUDA, "occupancy query failed for block size %d", block);
+    const int cap_bps = env_int("PFG_BLOCKS_PER_SM", 0);
+    if (cap_bps > 0) bps = std::min(bps, cap_bps);
+    const int grid = s->sm_count * bps;
+
+    if (timed) PFG_CUDA(cudaEventRecord(s->ev0, s->stream));
+    if (h_srcs) {
+        memcpy(s->h_srcs, h_srcs, (size_t)k * 4);
+        PFG_CUDA(cudaMemcpyAsync(s->d_srcs, s->h_srcs, (size_t)k * 4, cudaMemcpyHostToDevice, s->stream));
+    }
+    PFG_CUDA(cudaMemcpyAsync(s->d_ctl, c, run_bytes, cudaMemcpyHostToDevice, s->stream));
+    cudaError_t le = launch_persistent(p, astar != 0, o.atomic, map, block, grid, s->stream);
+    if (le != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PFG_ERR_CUDA, "persistent launch failed (grid %d x %d): %s", grid, block,
+                    cudaGetErrorString(le));
+    }
+    if (timed) PFG_CUDA(cudaEventRecord(s->ev1, s->stream));
+    PFG_CUDA(cudaMemcpyAsync(c, s->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream));
+    s->pending = true;
+    s->last_mode = mode;
+    s->last_delta = delta;
+    s->last_k = k;
+    return PFG_OK;
+}
+
+// Waits for the enqueued run and converts its control block into stats/status.
+static pfg_status complete_run(pfg_solver* s, pfg_stats* stats_out) {
+    if (!s->pending) return fail(PFG_ERR_INVALID_ARGUMENT, "no run in flight");
+    s->pending = false;
+    PFG_CUDA(cudaStreamSynchronize(s->stream));
+    const Ctl* c = s->h_ctl;
+    s->epoch_hint = std::max({c->near_epoch, c->far_epoch, c->r_epoch});
+    if (stats_out) {
+        memset(stats_out, 0, sizeof(*stats_out));
+        stats_out->edges_scanned = c->stats[0];
+        stats_out->atomics_issued = c->stats[1];
+        stats_out->updates = c->stats[2];
+        stats_out->pushes = c->stats[3];
+        stats_out->iterations = c->iterations;
+        stats_out->host_syncs = 1;
+        stats_out->launches = 1;
+        stats_out->buckets = s->last_mode == MODE_DELTA ? c->buckets : 0u;
+        stats_out->delta = s->last_delta;
+        stats_out->rounds = c->rounds;
+    }
+    if (c->status == DS_TIMEOUT) {
+        // A wait gave up: reset the naive masks so the next run starts clean.
+        const u64 words = (u64)s->n / 32 + 1;
+        for (int i = 0; i < 2; ++i) cudaMemsetAsync(s->d_naive[i], 0, words * 4, s->stream);
+        cudaStreamSynchronize(s->stream);
+        return fail(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
+    }
+    if (c->status == DS_NOT_CONVERGED) {
+        const u64 words = (u64)s->n / 32 + 1;
+        for (int i = 0; i < 2; ++i) cudaMemsetAsync(s->d_naive[i], 0, words * 4, s->stream);
+        cudaStreamSynchronize(s->stream);
+        const char* what = s->last_mode == MODE_NAIVE ? "Naive relaxation"
+                         : s->last_mode == MODE_FRONTIER ? "Frontier relaxation" : "Delta-stepping";
+        return fail(PFG_ERR_NOT_CONVERGED, "%s did not converge", what);
+    }
+    if (c->status == DS_BAD_SOURCE) return fail(PFG_ERR_INVALID_ARGUMENT, "source out of range");
+    if (c->status != DS_OK) return fail(PFG_ERR_CUDA, "device status %u", c->status);
+    return PFG_OK;
+}
+
+extern "C" pfg_status pfg_run(pfg_solver* s, const uint32_t* h_srcs, uint32_t k, int32_t astar,
+                              uint32_t dst, const pfg_options* opt, pfg_stats* stats_out,
+                              uint64_t* h_state_out, float* ms_out) {
+    if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
+    if (!h_srcs) return fail(PFG_ERR_INVALID_ARGUMENT, "sources are NULL");
+    if (s->pending) {
+        pfg_status st = complete_run(s, nullptr);
+        (void)st;
+    }
+    pfg_status st = enqueue_run(s, h_srcs, nullptr, k, astar, dst, opt, true);
+    if (st != PFG_OK) return st;
+    st = complete_run(s, stats_out);
+    if (st != PFG_OK) return st;
+    if (ms_out) {
+        float ms = 0.f;
+        PFG_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+        *ms_out = ms;
+    }
+    if (h_state_out) {
+        PFG_CUDA(cudaMemcpyAsync(h_state_out, s->d_state, (size_t)k * s->n * 8,
+                                 cudaMemcpyDeviceToHost, s->stream));
+        PFG_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    return PFG_OK;
+}
+
+extern "C" pfg_status pfg_run_async(pfg_solver* s, const uint32_t* d_srcs, uint32_t k,
+                                    int32_t astar, uint32_t dst, const pfg_options* opt) {
+    if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
+    if (!d_srcs) return fail(PFG_ERR_INVALID_ARGUMENT, "sources are NULL");
+    if (s->pending) {
+        pfg_status st = complete_run(s, nullptr);
+        (void)st;
+    }
+    return enqueue_run(s, nullptr, d_srcs, k, astar, dst, opt, false);
+}
+
+extern "C" pfg_status pfg_finish(pfg_solver* s, pfg_stats* stats_out) {
+    if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
+    return complete_run(s, stats_out);
+}
+
+extern "C" pfg_status pfg_copy_state(pfg_solver* s, uint64_t first, uint64_t count, uint64_t* h_out) {
+    if (!s || !h_out) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (first + count > (u64)s->K * s->n) return fail(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
+    PFG_CUDA(cudaSetDevice(s->device));
+    if (s->pending) {
+        pfg_status st = complete_run(s, nullptr);
+        if (st != PFG_OK) return st;
+    }
+    PFG_CUDA(cudaMemcpyAsync(h_out, s->d_state + first, count * 8, cudaMemcpyDeviceToHost, s->stream));
+    PFG_CUDA(cudaStreamSynchronize(s->stream));
+    return PFG_OK;
+}
+
+extern "C" pfg_status pfg_extract_path(pfg_solver* s, uint32_t inst, uint32_t src, uint32_t dst,
+                                       uint32_t* h_path, uint32_t cap, uint32_t* path_len_out) {
+    if (!s || !path_len_out || (cap > 0 && !h_path)) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (inst >= s->K || src >= s->n || dst >= s->n)
+        return fail(PFG_ERR_INVALID_ARGUMENT, "instance, source or target out of range");
+    PFG_CUDA(cudaSetDevice(s->device));
+    if (s->pending) {
+        pfg_status st = complete_run(s, nullptr);
+        if (st != PFG_OK) return st;
+    }
+    const u32 dcap = std::min<u32>(cap, s->n + 1);
+    cudaError_t e = launch_extract_path(s->d_state, (u64)inst * s->n, s->n, src, dst, s->d_path,
+                                        s->n + 1, s->d_path_len, s->stream);
+    if (e != cudaSuccess) return fail(PFG_ERR_CUDA, "path kernel: %s", cudaGetErrorString(e));
+    u32 len = 0;
+    PFG_CUDA(cudaMemcpyAsync(&len, s->d_path_len, 4, cudaMemcpyDeviceToHost, s->stream));
+    PFG_CUDA(cudaStreamSynchronize(s->stream));
+    *path_len_out = 0;
+    if (len == 0) return PFG_OK;
+    if (len > dcap) {
+        *path_len_out = len;
+        return fail(PFG_ERR_CAPACITY, "path has %u vertices, buffer holds %u", len, cap);
+    }
+    std::vector<u32> rev(len);
+    PFG_CUDA(cudaMemcpy(rev.data(), s->d_path, (size_t)len * 4, cudaMemcpyDeviceToHost));
+    for (u32 i = 0; i < len; ++i) h_path[i] = rev[len - 1 - i];
+    *path_len_out = len;
+    return PFG_OK;
+}
+
+// Loads a learned-policy network (host PolicyNet image) into the solver.
+extern "C" pfg_status pfg_set_policy(pfg_solver* s, const float* params, uint64_t count) {
+    if (!s || !params) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (count * sizeof(float) != sizeof(PolicyNet))
+        return fail(PFG_ERR_INVALID_ARGUMENT, "policy image has %llu floats, expected %llu",
+                    (unsigned long long)count, (unsigned long long)(sizeof(PolicyNet) / sizeof(float)));
+    PFG_CUDA(cudaSetDevice(s->device));
+    PFG_CUDA(cudaMemcpy(s->d_net, params, sizeof(PolicyNet), cudaMemcpyHostToDevice));
+    s->has_net = true;
+    return PFG_OK;
+}
+
+extern "C" uint64_t pfg_policy_param_count(void) { return sizeof(PolicyNet) / sizeof(float); }

@@ -1,0 +1,144 @@
+"""GPU parity of SSSP / A* / multi-source against the oracle (bit-exact).
+
+dist must equal the reference's cpuDijkstra; parent must equal the canonical
+smallest-index tight predecessor (the value the packed (dist<<32|parent)
+atomicMin converges to); every run must also pass the reference's three
+verifySSSP checks. A* must return cpuDijkstra's target distance and a valid
+path of that cost (A* parents are schedule dependent, so they are not compared).
+"""
+import itertools
+
+import numpy as np
+import pytest
+
+import pathfinding_gpu_b200 as pf
+from pathfinding_gpu_b200 import GpuAlgo, GpuOptions, Mapping, AtomicMode, Compaction
+
+pytestmark = pytest.mark.gpu
+
+SEED = 2026
+
+
+@pytest.fixture(scope="module")
+def grid100():
+    return pf.grid(100, 100, SEED)
+
+
+@pytest.fixture(scope="module")
+def grid100_solver(grid100):
+    s = pf.GpuSolver(grid100, 17)
+    yield s
+    s.close()
+
+
+@pytest.fixture(scope="module")
+def rmat12():
+    return pf.rmat(12, 16, seed=SEED)
+
+
+@pytest.fixture(scope="module")
+def rmat12_solver(rmat12):
+    s = pf.GpuSolver(rmat12, 8)
+    yield s
+    s.close()
+
+
+def sources_c0(g):
+    # source 0 plus 16 uniform sources from the seed
+    return [0] + pf.uniform_vertices(g.n, 16, SEED).tolist()
+
+
+def check_sssp(oracle, g, src, res):
+    d_ref, p_can = oracle.sssp_canonical(g, src)
+    assert np.array_equal(res.dist, d_ref), f"dist mismatch from {src}: {np.flatnonzero(res.dist != d_ref)[:5]}"
+    assert np.array_equal(res.parent, p_can), f"parent mismatch from {src}: {np.flatnonzero(res.parent != p_can)[:5]}"
+    rep = oracle.verify_sssp(g, src, d_ref, res.dist, res.parent, 64, src)
+    assert rep["errors"] == 0, rep
+
+
+ALGOS = [GpuAlgo.DeltaStep, GpuAlgo.Frontier, GpuAlgo.NaiveRelax]
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_grid100_all_sources(oracle, grid100, grid100_solver, algo):
+    for src in sources_c0(grid100):
+        res = grid100_solver.sssp(src, GpuOptions(algo=algo))
+        check_sssp(oracle, grid100, src, res)
+
+
+@pytest.mark.parametrize("mapping,atomic", list(itertools.product(list(Mapping), list(AtomicMode))))
+def test_grid100_variants(oracle, grid100, grid100_solver, mapping, atomic):
+    for algo in (GpuAlgo.DeltaStep, GpuAlgo.Frontier):
+        res = grid100_solver.sssp(77, GpuOptions(algo=algo, mapping=mapping, atomic=atomic))
+        check_sssp(oracle, grid100, 77, res)
+
+
+@pytest.mark.parametrize("delta", [1, 7, 60, 100, 120, 149, 150, 1000, 100000])
+def test_grid100_delta_sweep(oracle, grid100, grid100_solver, delta):
+    res = grid100_solver.sssp(4321, GpuOptions(delta=delta))
+    check_sssp(oracle, grid100, 4321, res)
+    assert res.stats.delta == delta
+
+
+def test_grid100_prefix_scan(oracle, grid100, grid100_solver):
+    res = grid100_solver.sssp(5, GpuOptions(algo=GpuAlgo.Frontier, compaction=Compaction.PrefixScan))
+    check_sssp(oracle, grid100, 5, res)
+
+
+@pytest.mark.parametrize("block", [32, 64, 128, 256, 512, 1024, 100])
+def test_grid100_block_sizes(oracle, grid100, grid100_solver, block):
+    res = grid100_solver.sssp(9999, GpuOptions(blockSize=block))
+    check_sssp(oracle, grid100, 9999, res)
+
+
+def test_grid100_astar(oracle, grid100, grid100_solver):
+    rng = pf.SplitMix64(SEED + 5)
+    for _ in range(24):
+        s, t = rng.below(grid100.n), rng.below(grid100.n)
+        d_ref, _, _, _ = oracle.dijkstra(grid100, s)
+        d_a, path_a, _, _ = oracle.astar(grid100, s, t)
+        assert d_a == d_ref[t]
+        for algo in ALGOS:
+            r = grid100_solver.astar(s, t, GpuOptions(algo=algo))
+            assert r.targetDist == d_ref[t], (s, t, algo)
+            assert oracle.validate_path(grid100, r.path, s, t, int(d_ref[t])), (s, t, algo)
+
+
+def test_grid100_multisource(oracle, grid100, grid100_solver):
+    srcs = sources_c0(grid100)
+    for algo in (GpuAlgo.DeltaStep, GpuAlgo.Frontier):
+        stats, ms, state = grid100_solver.run_state(srcs, GpuOptions(algo=algo))
+        dist, parent = pf.unpack(state)
+        dist = dist.reshape(len(srcs), -1)
+        parent = parent.reshape(len(srcs), -1)
+        for i, s in enumerate(srcs):
+            d_ref, p_can = oracle.sssp_canonical(grid100, s)
+            assert np.array_equal(dist[i], d_ref), (algo, i)
+            assert np.array_equal(parent[i], p_can), (algo, i)
+
+
+def test_rmat_variants(oracle, rmat12, rmat12_solver):
+    srcs = pf.pick_sources(rmat12, 4, SEED)
+    for algo, mapping in itertools.product(ALGOS, list(Mapping)):
+        for s in srcs[:2]:
+            res = rmat12_solver.sssp(int(s), GpuOptions(algo=algo, mapping=mapping))
+            check_sssp(oracle, rmat12, int(s), res)
+
+
+def test_rmat_small_delta_heavy_phase(oracle, rmat12, rmat12_solver):
+    # Delta below the max weight exercises the R set and heavy rounds
+    for delta in (1, 16, 64, 200):
+        res = rmat12_solver.sssp(int(pf.pick_sources(rmat12, 1, 7)[0]), GpuOptions(delta=delta))
+        check_sssp(oracle, rmat12, int(pf.pick_sources(rmat12, 1, 7)[0]), res)
+        assert res.stats.buckets >= 1
+
+
+def test_errors_like_reference(grid100_solver):
+    with pytest.raises(RuntimeError):
+        grid100_solver.sssp(10**6, GpuOptions())
+    with pytest.raises(RuntimeError):
+        grid100_solver.astar(0, 10**6, GpuOptions())
+    with pytest.raises(RuntimeError):
+        grid100_solver.multiSource(list(range(18)), GpuOptions(), None)
+    # the solver stays usable after an error
+    assert grid100_solver.sssp(0, GpuOptions()).dist[0] == 0
