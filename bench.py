@@ -1,0 +1,415 @@
+"""Benchmark of the SSSP hot path: batched Delta-stepping on the 1000 x 1000 grid road graph.
+
+One step = one multi-source SSSP launch (reference GpuSolver::multiSource,
+src/gpu_sssp.cu:553-569): K sources on the 1000x1000 grid (n = 10^6,
+m = 3,996,000 arcs, w = llround(100 * U[1, 1.5)), seed 2026) relaxed by one
+persistent kernel, fixed automatic Delta. Metric: GTEPS = reachable arcs of all
+K instances / step time (the reference's TEPS definition, src/main.cpp:209-213,
+aggregated over the batch).
+
+  value  device time of the step with the graph, sources and working set resident
+         in HBM (CUDA events on the solver's stream, L2 flushed between steps)
+  e2e    the same step through the C ABI pfg_run with host buffers: H2D of the K
+         sources from pinned memory, the run, and D2H of the K*n packed state
+         words into pinned memory, timed on the device
+  --impl reference   the reference's own cpuMultiSource (OpenMP, every host thread)
+         on the same graph and sources, compiled from its sources into oracle/_ref
+
+Multi-GPU: replicas (each rank runs its own batch of sources; no collective on the
+data path), value = all ranks' arcs / max step time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+GRID_SIDE = 1000
+SEED = 2026
+BATCH = 64
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--no-extras", action="store_true", help="skip the single-source / A* extras")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU, torchrun env)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, n):
+        import torch
+        self.torch = torch
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key: str):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(kernel_key)
+    except Exception:
+        return None
+
+
+def workload(rank: int, batch: int):
+    import pathfinding_gpu_b200 as pf
+    g = pf.grid(GRID_SIDE, GRID_SIDE, SEED)
+    srcs = pf.uniform_vertices(g.n, batch, SEED + 1000 * rank)
+    return g, srcs
+
+
+def reachable_stats(g, dist_rows):
+    """Reachable arcs and vertices summed over instances."""
+    deg = np.diff(g.row_offsets).astype(np.int64)
+    mr = nr = 0
+    for d in dist_rows:
+        r = d != 0xFFFFFFFF
+        nr += int(r.sum())
+        mr += int(deg[r].sum())
+    return mr, nr
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+def run_ours(args, D: "Dist"):
+    import torch
+    import pathfinding_gpu_b200 as pf
+    from pathfinding_gpu_b200 import GpuOptions
+
+    torch.cuda.set_device(D.local)
+    g, srcs = workload(D.rank, args.batch)
+    K = args.batch
+    solver = pf.GpuSolver(g, K, device=D.local)
+    stream = torch.cuda.ExternalStream(solver.stream(), device=D.local)
+    opt = GpuOptions()
+    lib = solver._lib
+    import ctypes as C
+    from pathfinding_gpu_b200 import _native as N
+
+    d_srcs = torch.from_numpy(srcs.astype(np.int32)).to(f"cuda:{D.local}")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{D.local}")
+    copt = opt.to_c()
+
+    def device_step():
+        N.check(lib.pfg_run_async(solver.handle, C.c_void_p(d_srcs.data_ptr()), K, 0, 0, C.byref(copt)))
+
+    def finish():
+        st = N.PfgStats()
+        N.check(lib.pfg_finish(solver.handle, C.byref(st)))
+        return st
+
+    # reachable arcs from one full run (also a parity spot check against the oracle on rank 0)
+    stats0, _, state = solver.run_state(srcs, opt)
+    dist, _ = pf.unpack(state)
+    dist = dist.reshape(K, g.n)
+    m_r, n_r = reachable_stats(g, dist)
+
+    for _ in range(args.warmup):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        device_step()
+        finish()
+    D.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    launches = 0
+    with ClockSampler(D.local) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()  # L2 flush between timed steps (256 MB > 126 MB L2)
+                evs[i][0].record(stream)
+            device_step()
+            launches += 1
+            evs[i][1].record(stream)
+            finish()
+        torch.cuda.synchronize()
+    D.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    local_total = sum(step_ms)
+    total_ms = D.max(local_total)
+    ms_per_step = total_ms / args.steps
+    arcs_all = D.sum(float(m_r))
+    value = arcs_all / (ms_per_step * 1e-3) / 1e9
+
+    # ---- roofline of the persistent kernel (one launch per step) ----
+    bytes_alg = 16.0 * m_r + 20.0 * n_r
+    achieved = bytes_alg / (statistics.mean(step_ms) * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic("k_persistent_grid1000_k64")
+
+    # ---- end to end through the C ABI with host buffers ----
+    h_state = torch.empty(K * g.n, dtype=torch.int64).pin_memory()
+    h_srcs = np.ascontiguousarray(srcs, np.uint32)
+    st = N.PfgStats()
+    ms_c = C.c_float()
+    e2e_evs = []
+    for i in range(args.warmup + args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        N.check(lib.pfg_run(solver.handle, N.ptr(h_srcs, N.u32), K, 0, 0, C.byref(copt), C.byref(st),
+                            C.cast(C.c_void_p(h_state.data_ptr()), C.POINTER(C.c_uint64)), C.byref(ms_c)))
+        b.record(stream)
+        if i >= args.warmup:
+            e2e_evs.append((a, b))
+    torch.cuda.synchronize()
+    e2e_ms = D.max(sum(a.elapsed_time(b) for a, b in e2e_evs) / len(e2e_evs))
+    e2e_value = arcs_all / (e2e_ms * 1e-3) / 1e9
+    # the copied-back result must be the device result
+    got = (h_state.numpy().view(np.uint64) >> np.uint64(32)).astype(np.uint32).reshape(K, g.n)
+    assert np.array_equal(got, dist), "e2e result differs from the device-resident run"
+
+    result = {
+        "metric": "GTEPS (reachable arcs / s, SSSP Delta-stepping, batch of sources)",
+        "value": round(value, 4), "unit": "GTEPS", "n_gpus": D.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"grid{GRID_SIDE}x{GRID_SIDE} multiSource K={K} Delta-stepping",
+                   "graph": f"grid {GRID_SIDE}x{GRID_SIDE}, 4-neighbour arcs both ways, "
+                            f"w=llround(100*U[1,1.5)), seed {SEED}",
+                   "n": g.n, "m": g.m, "batch": K, "delta": stats0.delta, "algo": "DeltaStep",
+                   "mapping": "Hybrid", "atomic": "MinRBA", "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"replicas x{D.world}"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 5), "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "bytes_alg_per_launch": bytes_alg,
+                     "bytes_model": "16 B per reachable arc + 20 B per reachable vertex, per instance"},
+        "e2e": {"value": round(e2e_value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 4 * K + 256,
+                "d2h_bytes_per_step": 8 * K * g.n + 256, "ms_per_step": round(e2e_ms, 4),
+                "api": "pfg_run (C ABI) with pinned host buffers"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "stats": {"rounds": stats0.rounds, "buckets": stats0.buckets,
+                  "edges_scanned": stats0.edgesScanned, "work_per_m": stats0.edgesScanned / max(1, m_r),
+                  "atomics": stats0.atomicsIssued},
+    }
+    solver.close()
+    return result, g, srcs
+
+
+def cpu_baseline(g, srcs, sample: int):
+    """The reference's cpuMultiSource (every host thread) on a bounded sample."""
+    from oracle import oracle as O
+    srcs = np.asarray(srcs[:sample], np.uint32)
+    if O.ref_available():
+        R = O.RefGraph.wrap(g)
+        ms, _, edges = R.multi_source(srcs, 0, False)
+        threads = O.ref().ref_max_threads()
+        kind = "reference"
+    else:
+        ms, _, edges = O.multi_source(g, srcs, 0, False)
+        threads = O.max_threads()
+        kind = "port"
+    deg = np.diff(g.row_offsets).astype(np.int64)
+    # grid graphs are strongly connected: every arc is reachable from every source
+    m_r = int(deg.sum()) * len(srcs)
+    return {"value": round(m_r / (ms * 1e-3) / 1e9, 4), "unit": "GTEPS", "cores": int(threads),
+            "kind": kind, "ms": round(ms, 2),
+            "sample": f"{len(srcs)} of the step's sources, cpuMultiSource OpenMP x{threads}"}
+
+
+def extras(g):
+    """Single-source modes and A* pairs on the same graph (reported beside the headline)."""
+    import pathfinding_gpu_b200 as pf
+    from pathfinding_gpu_b200 import GpuOptions, GpuAlgo
+    s = pf.GpuSolver(g, 1)
+    out = {}
+    src = int(pf.uniform_vertices(g.n, 1, SEED)[0])
+    for algo in (GpuAlgo.DeltaStep, GpuAlgo.Frontier, GpuAlgo.NaiveRelax):
+        s.run_state([src], GpuOptions(algo=algo), copy=False)
+        ts = [s.run_state([src], GpuOptions(algo=algo), copy=False)[1] for _ in range(3)]
+        out[f"sssp_{algo.name}_ms"] = round(statistics.median(ts), 3)
+    pairs = pf.uniform_vertices(g.n, 2 * 32, SEED + 7).reshape(-1, 2)
+    t0 = time.perf_counter()
+    tot = 0.0
+    for a, b in pairs:
+        _, ms, _ = s.run_state([int(a)], GpuOptions(), astar=True, dst=int(b), copy=False)
+        tot += ms
+    out["astar_32_pairs_mean_ms"] = round(tot / len(pairs), 3)
+    s.close()
+    return out
+
+
+def run_reference(args, D: "Dist"):
+    if D.rank != 0:
+        return None
+    import pathfinding_gpu_b200 as pf
+    from oracle import oracle as O
+    g, srcs = workload(0, args.batch)
+    K = args.batch
+    if O.ref_available():
+        R = O.RefGraph.wrap(g)
+        run = lambda s: R.multi_source(s, 0, False)
+        threads = O.ref().ref_max_threads()
+        kind = "reference"
+    else:
+        run = lambda s: O.multi_source(g, s, 0, False)
+        threads = O.max_threads()
+        kind = "port"
+    sample = min(K, max(threads, 8))
+    sub = np.asarray(srcs[:sample], np.uint32)
+    for _ in range(args.warmup):
+        run(sub[: max(1, threads)])
+    times = []
+    for _ in range(args.steps):
+        ms, _, _ = run(sub)
+        times.append(ms)
+    ms_step = statistics.mean(times)
+    m_r = g.m * sample
+    value = m_r / (ms_step * 1e-3) / 1e9
+    return {
+        "impl": "reference",
+        "metric": "GTEPS (reachable arcs / s, SSSP Delta-stepping, batch of sources)",
+        "value": round(value, 4), "unit": "GTEPS", "n_gpus": D.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"grid{GRID_SIDE}x{GRID_SIDE} multiSource K={K} Delta-stepping",
+                   "n": g.n, "m": g.m, "batch": K, "cpu_sources_per_step": sample},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": int(threads), "kind": kind,
+                         "sample": f"{sample} sources per step, cpuMultiSource OpenMP x{threads}"},
+        "e2e": {"value": round(value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    D = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            res = run_reference(args, D)
+            if D.rank == 0 and res is not None:
+                print(json.dumps(res))
+            return
+        res, g, srcs = run_ours(args, D)
+        if D.rank == 0:
+            if D.world == 1:
+                res["cpu_baseline"] = cpu_baseline(g, srcs, min(args.batch, 16))
+            if not args.no_extras:
+                res["extras"] = extras(g)
+            print(json.dumps(res))
+    finally:
+        D.close()
+
+
+if __name__ == "__main__":
+    main()

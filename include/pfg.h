@@ -73,6 +73,8 @@ typedef struct pfg_options {
                             on the device, so the host synchronizes once per run */
     int32_t compaction;  /* enum pfg_compaction (Frontier only)                   */
     int32_t policy;      /* enum pfg_policy_kind (Delta-stepping only)            */
+    int32_t eager;       /* Hybrid mapping: in-round propagation sub-rounds per
+                            grid round; -1 = engine default, 0 = off (extension) */
 } pfg_options;
 
 /* Mirrors GpuStats (reference: include/gpu_sssp.h:55-65) plus `rounds`. */

@@ -29,6 +29,7 @@ pfg_options to_c(const GpuOptions& o) {
     c.sync_every = o.syncEvery;
     c.compaction = static_cast<int32_t>(o.compaction);
     c.policy = PFG_POLICY_FIXED;
+    c.eager = -1;
     return c;
 }
 

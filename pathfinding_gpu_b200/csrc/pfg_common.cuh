@@ -52,45 +52,49 @@ enum CounterSlot : u32 { C_NEAR0 = 0, C_NEAR1 = 1, C_FAR0 = 2, C_FAR1 = 3, C_R =
 // Device status words (match pfg_status values).
 enum DevStatus : u32 { DS_OK = 0, DS_BAD_SOURCE = 1, DS_NOT_CONVERGED = 4, DS_TIMEOUT = 5 };
 
-// Control block in device memory. The part up to `persist` is rewritten by
-// the host before every run; the epoch counters below it carry over from run
-// to run so that stamp words never have to be cleared.
-struct Ctl {
-    // --- per run ---
-    u32 bar_count;     // grid barrier arrivals
-    u32 bar_gen;       // grid barrier generation
-    u32 phase;
-    u32 in_count;      // items in this round's input
-    u32 in_buf;        // near buffer read by a LIGHT round
-    u32 far_in;        // far pile scanned by a SCAN round
-    u32 far_out;       // far pile that receives pushes
-    u32 status;        // DevStatus
+// Round descriptor: everything a CTA needs to run the next round. Written by
+// the transition, read by every CTA with five 16-byte loads after a barrier.
+struct __align__(16) Rd {
+    u32 phase, in_count, in_buf, far_in;   // input of the round
+    u32 far_out, status, delta, heavy;     // far pile receiving pushes, Delta of the bucket
+    u32 near_epoch, far_epoch, r_epoch, naive_in;  // dedup stamps of this round's outputs
+    u32 flag_epoch, map_mode, pad0, pad1;
+    u64 lo, hi;                            // bucket window [lo, hi) on the key
+};
+
+// Control block in device memory (16-byte aligned, a multiple of 16 bytes so
+// the CTA running a transition loads and stores it with vector accesses).
+// The host rewrites everything before `persist` before each run; the epoch
+// counters after it carry over from run to run so stamp words never need
+// clearing.
+struct __align__(16) Ctl {
+    u32 bar_count;     // barrier tickets taken in this run (grows by gridDim.x per barrier)
+    u32 bar_gen;       // barriers completed in this run
+    u32 pad_b0, pad_b1;
+    Rd rd;
     u32 rounds;        // barrier epochs so far
     u32 iterations;    // rounds with a non-empty input
     u32 buckets;
     u32 round_cap;
-    u32 delta;         // Delta of the current bucket
     u32 delta0;        // Delta of the first bucket
-    u32 heavy;         // nonzero when some arc is heavier than Delta
     u32 changed;       // naive mode: some distance decreased this round
-    u32 naive_in;      // naive mode: which activity mask is read
     u32 policy_calls;  // learned-policy decisions taken
-    u64 lo, hi;        // current bucket window [lo, hi) on the key
+    u32 bucket_near;   // items entering the current bucket (policy feature)
+    u32 bucket_rounds; // rounds spent in the current bucket (policy feature)
+    u32 pad_c0, pad_c1, pad_c2;
     u64 far_min[2];    // smallest key pushed to each far pile
     u32 cnt[C_COUNT];  // queue tails
     unsigned long long stats[4];  // edges, atomics, updates, pushes
-    u32 bucket_near;   // items entering the current bucket (policy feature)
-    u32 bucket_rounds; // rounds spent in the current bucket (policy feature)
     u64 bucket_edges;  // edges scanned up to the start of the bucket (policy feature)
     u64 bucket_edges_acc;  // edges scanned so far, flushed every round when the policy runs
-    u32 flag_epoch;    // prefix-scan mode: stamp of the flagged vertices
-    u32 pad_run;
     // --- persistent across runs ---
-    u32 persist;       // marker: everything below survives between runs
-    u32 near_epoch;    // stamp written by near pushes of the current round
-    u32 far_epoch;     // stamp of the far pile that receives pushes
-    u32 r_epoch;       // stamp of the current R set
+    u32 persist;       // marker: everything from here on survives between runs
+    u32 near_epoch;    // last stamp used by near pushes
+    u32 far_epoch;     // last stamp used by far pushes
+    u32 r_epoch;       // last stamp used by R pushes
 };
+static_assert(sizeof(Ctl) % 16 == 0, "Ctl must be a multiple of 16 bytes");
+static_assert(sizeof(Rd) == 80, "Rd layout");
 
 // Learned Delta-policy network (3 hidden layers of 64, fp32).
 constexpr int POL_IN = 12;
@@ -135,6 +139,8 @@ struct RunParams {
     int mode;          // RunMode
     int prefix_scan;   // 1: flag + scan compaction instead of queue pushes
     int policy;        // 1: learned Delta policy picks each bucket's Delta
+    u32 eager;         // hybrid mapping: eager sub-rounds per round (0 = off)
+    u32 eager_max_items;  // ... only in rounds whose input has at most this many items
     const PolicyNet* net;
     u64 timeout_ns;    // bound on every device-side wait
 };
@@ -205,9 +211,10 @@ __device__ __forceinline__ bool relax_state(u64* addr, u32 nd, u32 parent, u32& 
     }
 }
 
-// Claims item i for epoch e: true exactly once per (i, e).
+// Claims item i for epoch e: true exactly once per (i, e). A single exchange
+// (no read first): the stamp is almost never set already, and on the latency
+// path one L2 round trip matters more than an occasional redundant atomic.
 __device__ __forceinline__ bool claim_stamp(u32* stamp, u32 i, u32 e) {
-    if (ld_cg(stamp + i) == e) return false;
     return atomicExch(stamp + i, e) != e;
 }
 

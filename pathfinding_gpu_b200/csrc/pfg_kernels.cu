@@ -36,19 +36,17 @@ enum Kind { K_LIGHT = 0, K_SCAN = 1, K_HEAVY = 2 };
 // Multipliers of the automatic Delta that the learned policy chooses from.
 __constant__ float kPolicyMult[POL_OUT] = {0.25f, 0.5f, 1.f, 2.f, 4.f, 8.f, 16.f, 64.f};
 
-// Control-block snapshot, refreshed in shared memory after every barrier.
-struct Snap {
-    u32 phase, in_count, in_buf, far_in, far_out, status, delta, heavy;
-    u32 near_epoch, far_epoch, r_epoch, naive_in, map_mode, flag_epoch;
-    u64 lo, hi;
-};
+// The round descriptor, copied to shared memory after every barrier.
+typedef Rd Snap;
 
 struct Local {
     u32 edges = 0, atomics = 0, updates = 0, pushes = 0;
     u64 fmin = ~0ull;  // smallest key this thread pushed to the far pile this round
 };
 
-// Shared memory of the CTA-cooperative (scan-based) tier of the hybrid mapping.
+constexpr u32 CL_CAP = 2048;  // claimed-list entries per CTA (hybrid mapping)
+
+// Shared memory of the edge-balanced hybrid mapping.
 struct Coop {
     u32 off[MAX_BS + 1];
     u32 eb[MAX_BS];
@@ -57,6 +55,9 @@ struct Coop {
     u32 ib[MAX_BS];
     u32 ub[MAX_BS];
     u32 wsum[32];
+    u32 cl[CL_CAP];  // near vertices claimed by this CTA in the current round
+    u32 cl_n;        // entries appended (may exceed CL_CAP; the excess went to the global queue)
+    u32 cl_base;
 };
 
 // ---------------------------------------------------------------------------
@@ -127,9 +128,13 @@ __device__ __forceinline__ u32 light_end(const uint2* adj, u32 r0, u32 r1, u32 d
 // ---------------------------------------------------------------------------
 // Relaxation of one arc (u -> v, w) and queueing of the improved head.
 // ---------------------------------------------------------------------------
+// cl != nullptr (hybrid mapping): a claimed near vertex goes to the CTA's
+// claimed list in shared memory, which is relaxed again in the same round
+// (eager sub-rounds) and flushed to the global near queue at the end of the
+// round; only overflow goes to the global queue directly.
 template <bool ASTAR, int AM>
 __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32 u, u32 du,
-                                          u32 ib, u32 ub, u32 v, u32 w, Local& L) {
+                                          u32 ib, u32 ub, u32 v, u32 w, Local& L, Coop* cl) {
     if (w == PAD_W) return;
     L.edges++;
     const u64 nd = (u64)du + w;
@@ -150,9 +155,16 @@ __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32
     }
     if (key < s.hi) {
         if (claim_stamp(p.near_stamp, gv, s.near_epoch)) {
+            L.pushes++;
+            if (cl) {
+                const u32 slot = atomicAdd(&cl->cl_n, 1u);
+                if (slot < CL_CAP) {
+                    cl->cl[slot] = gv;
+                    return;
+                }
+            }
             const u32 out = s.in_buf ^ 1u;
             queue_push(p.nearq[out], &c->cnt[C_NEAR0 + out], gv);
-            L.pushes++;
         }
     } else {
         if (claim_stamp(p.far_stamp, gv, s.far_epoch)) {
@@ -171,9 +183,114 @@ __device__ __forceinline__ void relax_range_thread(const RunParams& p, const Sna
     const uint4* a4 = reinterpret_cast<const uint4*>(p.adj);
     for (u32 e = eb & ~1u; e < ee; e += 2) {
         const uint4 q = __ldg(a4 + (e >> 1));
-        if (e >= eb) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, q.x, q.y, L);
-        if (e + 1 < ee) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, q.z, q.w, L);
+        if (e >= eb) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, q.x, q.y, L, nullptr);
+        if (e + 1 < ee) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, q.z, q.w, L, nullptr);
     }
+}
+
+// Reads one input item (a state index) and decides what to relax: returns
+// false when the item is stale, pruned, or (SCAN) outside the new window -
+// items of a later bucket are carried to the next far pile here. On true,
+// [eb, ee) is the arc range of the round kind (light prefix / heavy suffix).
+template <bool ASTAR>
+__device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32 gi, int kind,
+                                          Local& L, u32& u, u32& ib, u32& du, u32& ub, u32& eb,
+                                          u32& ee) {
+    Ctl* c = p.ctl;
+    const u32 inst = p.k > 1 ? gi / p.n : 0u;
+    ib = inst * p.n;
+    u = gi - ib;
+    du = st_dist(ld_state(p.state + gi));
+    bool act = du != INF32;
+    u64 key = du;
+    if constexpr (ASTAR) {
+        ub = st_dist(ld_state(p.state + ib + p.target));
+        if (act) {
+            key += h_of(p, u);
+            if (key >= ub) act = false;
+        }
+    }
+    if (kind == K_SCAN && act) {
+        if (key < s.lo) {
+            act = false;  // settled in an earlier bucket (stale far entry)
+        } else if (key >= s.hi) {
+            act = false;  // belongs to a later bucket: keep it far
+            if (claim_stamp(p.far_stamp, gi, s.far_epoch)) {
+                queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gi);
+                L.pushes++;
+            }
+            L.fmin = key < L.fmin ? key : L.fmin;
+        }
+    }
+    if (!act) return false;
+    const u32 r0 = __ldg(p.prow + u), r1 = __ldg(p.prow + u + 1);
+    if (kind == K_HEAVY) {
+        eb = light_end(p.adj, r0, r1, s.delta);
+        ee = r1;
+    } else {
+        eb = r0;
+        ee = s.heavy ? light_end(p.adj, r0, r1, s.delta) : r1;
+        // R = vertices of this bucket that own real heavy arcs.
+        if (s.heavy && ee < r1 && __ldg(&p.adj[ee].y) != PAD_W) {
+            if (claim_stamp(p.r_stamp, gi, s.r_epoch)) {
+                queue_push(p.rq, &c->cnt[C_R], gi);
+                L.pushes++;
+            }
+        }
+    }
+    return ee > eb;
+}
+
+// Edge-balanced CTA mapping: the selected arcs of all items of a chunk are
+// numbered with a block-wide scan and dealt out one per thread, so every arc
+// of a road-graph vertex and every slice of a hub row is relaxed in parallel
+// (one dependent chain per arc). Called by every thread of the CTA.
+template <bool ASTAR, int AM>
+__device__ __forceinline__ void relax_chunk_edges(const RunParams& p, const Snap& s, bool act, u32 u,
+                                                  u32 du, u32 ib, u32 ub, u32 eb, u32 ee, Local& L,
+                                                  Coop& cs, Coop* cl) {
+    const u32 BS = blockDim.x;
+    u32 total = 0;
+    const u32 sz = act ? ee - eb : 0u;
+    const u32 off = block_exclusive_scan(sz, cs.wsum, total);
+    if (total == 0) return;  // block-uniform
+    cs.off[threadIdx.x] = off;
+    cs.eb[threadIdx.x] = eb;
+    cs.u[threadIdx.x] = u;
+    cs.du[threadIdx.x] = du;
+    cs.ib[threadIdx.x] = ib;
+    cs.ub[threadIdx.x] = ub;
+    if (threadIdx.x == 0) cs.off[BS] = total;
+    __syncthreads();
+    for (u32 j = threadIdx.x; j < total; j += BS) {
+        // owner = last slot with off <= j (zero-size slots repeat offsets, the
+        // last of them is the owner); fixed-trip search, no divergence
+        u32 lo = 0;
+#pragma unroll
+        for (u32 step = MAX_BS / 2; step > 0; step >>= 1) {
+            const u32 cand = lo + step;
+            if (cand < BS && cs.off[cand] <= j) lo = cand;
+        }
+        const u32 e = cs.eb[lo] + (j - cs.off[lo]);
+        const uint2 a = __ldg(p.adj + e);
+        relax_arc<ASTAR, AM>(p, s, cs.u[lo], cs.du[lo], cs.ib[lo], cs.ub[lo], a.x, a.y, L, cl);
+    }
+    __syncthreads();
+}
+
+// Writes the CTA's claimed list to the global near queue (one atomicAdd per CTA).
+__device__ __forceinline__ void flush_claimed(const RunParams& p, const Snap& s, Coop& cs) {
+    __syncthreads();
+    const u32 total = min(cs.cl_n, CL_CAP);
+    if (total > 0) {  // block-uniform
+        const u32 out = s.in_buf ^ 1u;
+        if (threadIdx.x == 0) cs.cl_base = atomicAdd(&p.ctl->cnt[C_NEAR0 + out], total);
+        __syncthreads();
+        u32* q = p.nearq[out] + cs.cl_base;
+        for (u32 i = threadIdx.x; i < total; i += blockDim.x) q[i] = cs.cl[i];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) cs.cl_n = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -183,58 +300,18 @@ template <bool ASTAR, int AM, int MAP>
 __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u32 count, int kind,
                             Local& L, Coop& cs) {
     const u32 BS = blockDim.x;
-    Ctl* c = p.ctl;
-    const bool split = s.heavy != 0;  // some arcs are heavier than Delta
-    for (u32 base = blockIdx.x * BS; base < count; base += gridDim.x * BS) {
+    // Hybrid mapping keeps claimed near vertices in shared memory (see relax_arc).
+    Coop* cl = (MAP == 2 && !p.prefix_scan) ? &cs : nullptr;
+    // Every CTA takes one contiguous slice of the input, so a small frontier is
+    // spread over all SMs (one arc chain per thread) instead of a few CTAs.
+    const u32 per = (count + gridDim.x - 1u) / gridDim.x;
+    const u32 sbeg = min(count, blockIdx.x * per);
+    const u32 send = min(count, sbeg + per);
+    for (u32 base = sbeg; base < send; base += BS) {
         const u32 idx = base + threadIdx.x;
         u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, ub = INF32;
         bool act = false;
-        if (idx < count) {
-            const u32 gi = ld_cg(in + idx);
-            const u32 inst = p.k > 1 ? gi / p.n : 0u;
-            ib = inst * p.n;
-            u = gi - ib;
-            du = st_dist(ld_state(p.state + gi));
-            act = du != INF32;
-            u64 key = du;
-            if constexpr (ASTAR) {
-                ub = st_dist(ld_state(p.state + ib + p.target));
-                if (act) {
-                    key += h_of(p, u);
-                    if (key >= ub) act = false;
-                }
-            }
-            if (kind == K_SCAN && act) {
-                if (key < s.lo) {
-                    act = false;  // settled in an earlier bucket (stale far entry)
-                } else if (key >= s.hi) {
-                    act = false;  // belongs to a later bucket: keep it far
-                    if (claim_stamp(p.far_stamp, gi, s.far_epoch)) {
-                        queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gi);
-                        L.pushes++;
-                    }
-                    L.fmin = key < L.fmin ? key : L.fmin;
-                }
-            }
-            if (act) {
-                const u32 r0 = __ldg(p.prow + u), r1 = __ldg(p.prow + u + 1);
-                if (kind == K_HEAVY) {
-                    eb = light_end(p.adj, r0, r1, s.delta);
-                    ee = r1;
-                } else {
-                    eb = r0;
-                    ee = split ? light_end(p.adj, r0, r1, s.delta) : r1;
-                    // R = vertices of this bucket that own real heavy arcs.
-                    if (split && ee < r1 && __ldg(&p.adj[ee].y) != PAD_W) {
-                        if (claim_stamp(p.r_stamp, gi, s.r_epoch)) {
-                            queue_push(p.rq, &c->cnt[C_R], gi);
-                            L.pushes++;
-                        }
-                    }
-                }
-                if (ee <= eb) act = false;
-            }
-        }
+        if (idx < send) act = take_item<ASTAR>(p, s, ld_cg(in + idx), kind, L, u, ib, du, ub, eb, ee);
 
         if constexpr (MAP == 0) {  // thread per item
             if (act) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, eb, ee, L);
@@ -249,37 +326,42 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
                 const u32 web = __shfl_sync(FULL, eb, leader), wee = __shfl_sync(FULL, ee, leader);
                 for (u32 e = web + lane; e < wee; e += 32) {
                     const uint2 a = __ldg(p.adj + e);
-                    relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, a.x, a.y, L);
+                    relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, a.x, a.y, L, nullptr);
                 }
             }
-        } else {  // hybrid: short rows by their own thread, long rows CTA-cooperative
-            const bool big = act && (ee - eb) >= COOP_MIN && s.map_mode != 0;
-            if (act && !big) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, eb, ee, L);
-            if (__syncthreads_or(big)) {
-                u32 total = 0;
-                const u32 sz = big ? ee - eb : 0u;
-                const u32 off = block_exclusive_scan(sz, cs.wsum, total);
-                cs.off[threadIdx.x] = off;
-                cs.eb[threadIdx.x] = eb;
-                cs.u[threadIdx.x] = u;
-                cs.du[threadIdx.x] = du;
-                cs.ib[threadIdx.x] = ib;
-                cs.ub[threadIdx.x] = ub;
-                if (threadIdx.x == 0) cs.off[BS] = total;
-                __syncthreads();
-                for (u32 j = threadIdx.x; j < total; j += BS) {
-                    // owner = last slot with off <= j (slots of size 0 repeat offsets)
-                    u32 lo = 0, hi = BS;
-                    while (lo < hi) {
-                        const u32 mid = (lo + hi + 1) >> 1;
-                        if (cs.off[mid] <= j) lo = mid; else hi = mid - 1;
+        } else {
+            relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, eb, ee, L, cs, cl);
+        }
+    }
+    if constexpr (MAP == 2) {
+        if (cl) {
+            // Eager sub-rounds: the vertices this CTA claimed for the next round
+            // (keys inside the bucket window) are relaxed again right away, so
+            // the wavefront advances several hops per grid barrier. They stay in
+            // the claimed list and reach the global near queue at the flush, so
+            // whatever happens here, the next round still processes them.
+            // Only latency-bound rounds (small inputs) propagate eagerly: on
+            // large frontiers the extra relaxations cost more than the barriers
+            // they save.
+            if (kind != K_HEAVY && count <= p.eager_max_items) {
+                u32 lo = 0;
+                for (u32 sub = 0; sub < p.eager; ++sub) {
+                    __syncthreads();
+                    const u32 hi = min(cs.cl_n, CL_CAP);
+                    __syncthreads();
+                    if (hi <= lo) break;  // block-uniform
+                    for (u32 base = lo; base < hi; base += BS) {
+                        const u32 idx = base + threadIdx.x;
+                        u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, ub = INF32;
+                        bool act = false;
+                        if (idx < hi)
+                            act = take_item<ASTAR>(p, s, cs.cl[idx], K_LIGHT, L, u, ib, du, ub, eb, ee);
+                        relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, eb, ee, L, cs, cl);
                     }
-                    const u32 e = cs.eb[lo] + (j - cs.off[lo]);
-                    const uint2 a = __ldg(p.adj + e);
-                    relax_arc<ASTAR, AM>(p, s, cs.u[lo], cs.du[lo], cs.ib[lo], cs.ub[lo], a.x, a.y, L);
+                    lo = hi;
                 }
-                __syncthreads();
             }
+            flush_claimed(p, s, cs);
         }
     }
 }
@@ -395,33 +477,37 @@ __device__ u32 policy_pick(const PolicyNet* net, const float* feat, float* act0,
 }
 
 // ---------------------------------------------------------------------------
-// Transition, run by the CTA that arrives last at a barrier (block-uniform
-// control flow; thread 0 owns the control block, the whole CTA evaluates the
-// policy network when a bucket advance asks for it).
+// Transition, run by the CTA that arrives last at a barrier, on a copy of the
+// control block in shared memory (block-uniform control flow; thread 0 owns
+// the logic, the whole CTA evaluates the policy network when a bucket advance
+// asks for it).
 // ---------------------------------------------------------------------------
-__device__ void transition(const RunParams& p, u32* s_flag, float* s_feat, float* act0,
+__device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_feat, float* act0,
                            float* act1) {
-    Ctl* c = p.ctl;
-    volatile Ctl* vc = c;
     const u32 t = threadIdx.x;
     // s_flag[0]: 0 = no bucket advance, 1 = advance with the policy, 2 = fixed Delta
     if (t == 0) {
+        Rd& r = sc.rd;
         s_flag[0] = 0;
-        const u32 ph = vc->phase;
-        const u32 rounds = vc->rounds;
-        const u32 old_near_epoch = vc->near_epoch;
-        const u32 in_buf = vc->in_buf;
+        const u32 ph = r.phase;
+        const u32 rounds = sc.rounds;
+        const u32 in_buf = r.in_buf;
         const u32 out = in_buf ^ 1u;
-        c->rounds = rounds + 1u;
-        c->near_epoch = old_near_epoch + 1u;  // every round pushes with a fresh stamp
-        c->bucket_rounds = vc->bucket_rounds + 1u;
+        const u32 old_near_epoch = r.near_epoch;
+        sc.rounds = rounds + 1u;
+        sc.bucket_rounds += 1u;
+        r.near_epoch = old_near_epoch + 1u;  // every round pushes with a fresh stamp
         bool advance = false;
-        if (vc->status != DS_OK) {
-            c->phase = PH_DONE;
-        } else if (rounds > vc->round_cap) {
-            c->status = DS_NOT_CONVERGED;
-            c->phase = PH_DONE;
+        if (r.status != DS_OK) {
+            r.phase = PH_DONE;
+        } else if (rounds > sc.round_cap) {
+            r.status = DS_NOT_CONVERGED;
+            r.phase = PH_DONE;
         } else if (ph == PH_INIT) {
+            // Stamps continue from the previous run.
+            r.near_epoch = sc.near_epoch + 1u;
+            r.far_epoch = sc.far_epoch + 1u;
+            r.r_epoch = sc.r_epoch + 1u;
             // Seed the k sources (reference seedKernel, src/gpu_kernels.cuh:340-352).
             bool bad = false;
             for (u32 i = 0; i < p.k; ++i) bad = bad || p.srcs[i] >= p.n;
@@ -430,112 +516,112 @@ __device__ void transition(const RunParams& p, u32* s_flag, float* s_feat, float
                 p.state[gi] = pack_state(0u, NO_PARENT);
                 if (p.mode != MODE_NAIVE) p.nearq[0][i] = gi;
             }
-            c->iterations = vc->iterations + 1u;
+            sc.iterations += 1u;
             if (bad) {
-                c->status = DS_BAD_SOURCE;  // sources given in device memory are checked here
-                c->phase = PH_DONE;
+                r.status = DS_BAD_SOURCE;  // sources given in device memory are checked here
+                r.phase = PH_DONE;
             } else if (p.mode == MODE_NAIVE) {
                 const u32 src = p.srcs[0];
                 atomicOr(p.naive_mask[0] + (src >> 5), 1u << (src & 31u));
-                c->naive_in = 0u;
-                c->changed = 0u;
-                c->in_count = p.n;
-                c->phase = PH_NAIVE;
+                r.naive_in = 0u;
+                sc.changed = 0u;
+                r.in_count = p.n;
+                r.phase = PH_NAIVE;
             } else {
                 u64 key0 = 0;
                 if (p.astar && p.use_h)
                     key0 = heuristic_value(p.x[p.srcs[0]], p.y[p.srcs[0]], p.xt, p.yt, p.hscale);
-                const u64 d = vc->delta;
-                c->cnt[C_NEAR0] = p.k;
-                c->cnt[C_NEAR1] = 0u;
-                c->in_buf = 0u;
-                c->in_count = p.k;
-                c->lo = 0ull;
-                c->hi = p.mode == MODE_FRONTIER ? ~0ull : (key0 / d + 1ull) * d;
-                c->bucket_near = p.k;
-                c->bucket_rounds = 0u;
-                c->phase = PH_LIGHT;
+                const u64 d = r.delta;
+                sc.cnt[C_NEAR0] = p.k;
+                sc.cnt[C_NEAR1] = 0u;
+                r.in_buf = 0u;
+                r.in_count = p.k;
+                r.lo = 0ull;
+                r.hi = p.mode == MODE_FRONTIER ? ~0ull : (key0 / d + 1ull) * d;
+                sc.bucket_near = p.k;
+                sc.bucket_rounds = 0u;
+                r.phase = PH_LIGHT;
             }
         } else if (ph == PH_NAIVE) {
-            c->iterations = vc->iterations + 1u;
-            if (vc->changed == 0u) {
-                c->phase = PH_DONE;
+            sc.iterations += 1u;
+            if (sc.changed == 0u) {
+                r.phase = PH_DONE;
             } else {
-                c->changed = 0u;
-                c->naive_in = vc->naive_in ^ 1u;
+                sc.changed = 0u;
+                r.naive_in ^= 1u;
             }
         } else if (ph == PH_COMPACT) {
-            const u32 nn = vc->cnt[C_NEAR0 + out];
+            const u32 nn = sc.cnt[C_NEAR0 + out];
             if (nn) {
-                c->cnt[C_NEAR0 + in_buf] = 0u;
-                c->in_buf = out;
-                c->in_count = nn;
-                c->iterations = vc->iterations + 1u;
-                c->phase = PH_LIGHT;
+                sc.cnt[C_NEAR0 + in_buf] = 0u;
+                r.in_buf = out;
+                r.in_count = nn;
+                sc.iterations += 1u;
+                r.phase = PH_LIGHT;
             } else {
-                c->phase = PH_DONE;
+                r.phase = PH_DONE;
             }
         } else if (ph == PH_LIGHT || ph == PH_SCAN) {
-            const u32 nn = vc->cnt[C_NEAR0 + out];
+            const u32 nn = sc.cnt[C_NEAR0 + out];
             if (p.prefix_scan) {
                 // the round just ended flagged its improved vertices with its stamp
-                c->flag_epoch = old_near_epoch;
-                c->cnt[C_NEAR0 + out] = 0u;
-                c->in_count = p.total;
-                c->phase = PH_COMPACT;
+                r.flag_epoch = old_near_epoch;
+                sc.cnt[C_NEAR0 + out] = 0u;
+                r.in_count = p.total;
+                r.phase = PH_COMPACT;
             } else if (nn) {
-                c->cnt[C_NEAR0 + in_buf] = 0u;
-                c->in_buf = out;
-                c->in_count = nn;
-                c->iterations = vc->iterations + 1u;
-                c->bucket_near = vc->bucket_near + nn;
-                c->phase = PH_LIGHT;
-            } else if (vc->heavy && vc->cnt[C_R]) {
-                c->in_count = vc->cnt[C_R];
-                c->iterations = vc->iterations + 1u;
-                c->phase = PH_HEAVY;
+                sc.cnt[C_NEAR0 + in_buf] = 0u;
+                r.in_buf = out;
+                r.in_count = nn;
+                sc.iterations += 1u;
+                sc.bucket_near += nn;
+                r.phase = PH_LIGHT;
+            } else if (r.heavy && sc.cnt[C_R]) {
+                r.in_count = sc.cnt[C_R];
+                sc.iterations += 1u;
+                r.phase = PH_HEAVY;
             } else {
                 advance = true;
             }
         } else if (ph == PH_HEAVY) {
-            c->cnt[C_R] = 0u;
-            c->r_epoch = vc->r_epoch + 1u;  // R may be refilled in this bucket (A*)
-            const u32 nn = vc->cnt[C_NEAR0 + out];
+            sc.cnt[C_R] = 0u;
+            r.r_epoch += 1u;  // R may be refilled in this bucket (A*)
+            const u32 nn = sc.cnt[C_NEAR0 + out];
             if (nn) {
-                c->cnt[C_NEAR0 + in_buf] = 0u;
-                c->in_buf = out;
-                c->in_count = nn;
-                c->iterations = vc->iterations + 1u;
-                c->phase = PH_LIGHT;
+                sc.cnt[C_NEAR0 + in_buf] = 0u;
+                r.in_buf = out;
+                r.in_count = nn;
+                sc.iterations += 1u;
+                r.phase = PH_LIGHT;
             } else {
                 advance = true;
             }
         }
         if (advance) {
-            c->buckets = vc->buckets + 1u;
-            const u32 fin = vc->far_out;
-            const u32 fn = vc->cnt[C_FAR0 + fin];
-            const u64 est = vc->far_min[fin];
+            sc.buckets += 1u;
+            const u32 fin = r.far_out;
+            const u32 fn = sc.cnt[C_FAR0 + fin];
+            const u64 est = sc.far_min[fin];
             if (fn == 0u || est == ~0ull) {
-                c->phase = PH_DONE;
+                r.phase = PH_DONE;
             } else {
                 s_flag[0] = p.policy ? 1u : 2u;
                 if (p.policy) {
                     const double aw = p.avg_w > 0.0 ? p.avg_w : 1.0;
-                    const u64 edges_now = vc->bucket_edges_acc;
+                    const u64 edges_now = sc.bucket_edges_acc;
                     s_feat[0] = log2f(1.f + (float)fn);
-                    s_feat[1] = log2f(1.f + (float)vc->bucket_near);
-                    s_feat[2] = log2f(1.f + (float)vc->bucket_rounds);
-                    s_feat[3] = (float)((double)(est - vc->hi) / aw);
-                    s_feat[4] = log2f(1.f + (float)(edges_now - vc->bucket_edges));
-                    s_feat[5] = log2f(1.f + (float)vc->buckets);
-                    s_feat[6] = log2f((float)((double)vc->delta / aw));
+                    s_feat[1] = log2f(1.f + (float)sc.bucket_near);
+                    s_feat[2] = log2f(1.f + (float)sc.bucket_rounds);
+                    s_feat[3] = (float)((double)(est - r.hi) / aw);
+                    s_feat[4] = log2f(1.f + (float)(edges_now - sc.bucket_edges));
+                    s_feat[5] = log2f(1.f + (float)sc.buckets);
+                    s_feat[6] = log2f((float)((double)r.delta / aw));
                     s_feat[7] = log2f(1.f + (float)p.avg_deg);
                     s_feat[8] = log2f((float)((double)p.maxw / aw));
                     s_feat[9] = log2f(1.f + (float)p.n);
                     s_feat[10] = (float)((double)est / (aw * sqrt((double)p.n)));
-                    s_feat[11] = fminf(1.f, (float)vc->delta / (float)(p.maxw ? p.maxw : 1u));
-                    c->bucket_edges = edges_now;
+                    s_feat[11] = fminf(1.f, (float)r.delta / (float)(p.maxw ? p.maxw : 1u));
+                    sc.bucket_edges = edges_now;
                 }
             }
         }
@@ -547,41 +633,52 @@ __device__ void transition(const RunParams& p, u32* s_flag, float* s_feat, float
         if (t == 0) s_flag[1] = cls;
     }
     __syncthreads();
-    if (t == 0 && need != 0u) {
-        // Open the next bucket: the far pile collected during this bucket is
-        // scanned against the window [old hi, new hi).
-        u32 d = p.delta;
-        if (need == 1u) {
-            const float dm = (float)p.delta * kPolicyMult[s_flag[1]];
-            d = dm < 1.f ? 1u : (dm > 2.0e9f ? 2000000000u : (u32)dm);
-            c->policy_calls = vc->policy_calls + 1u;
+    if (t == 0) {
+        Rd& r = sc.rd;
+        if (need != 0u) {
+            // Open the next bucket: the far pile collected during this bucket is
+            // scanned against the window [old hi, new hi).
+            u32 d = p.delta;
+            if (need == 1u) {
+                const float dm = (float)p.delta * kPolicyMult[s_flag[1]];
+                d = dm < 1.f ? 1u : (dm > 2.0e9f ? 2000000000u : (u32)dm);
+                sc.policy_calls += 1u;
+            }
+            const u32 fin = r.far_out;
+            const u64 est = sc.far_min[fin];
+            r.delta = d;
+            r.heavy = d < p.maxw ? 1u : 0u;
+            r.lo = r.hi;
+            r.hi = need == 1u ? est + d : (est / d + 1ull) * d;
+            r.far_in = fin;
+            r.far_out = fin ^ 1u;
+            sc.cnt[C_FAR0 + (fin ^ 1u)] = 0u;
+            sc.far_min[fin ^ 1u] = ~0ull;
+            r.far_epoch += 1u;
+            r.r_epoch += 1u;
+            r.in_count = sc.cnt[C_FAR0 + fin];
+            sc.iterations += 1u;
+            sc.bucket_near = 0u;
+            sc.bucket_rounds = 0u;
+            r.phase = PH_SCAN;
         }
-        const u32 fin = vc->far_out;
-        const u64 est = vc->far_min[fin];
-        c->delta = d;
-        c->heavy = d < p.maxw ? 1u : 0u;
-        c->lo = vc->hi;
-        c->hi = need == 1u ? est + d : (est / d + 1ull) * d;
-        c->far_in = fin;
-        c->far_out = fin ^ 1u;
-        c->cnt[C_FAR0 + (fin ^ 1u)] = 0u;
-        c->far_min[fin ^ 1u] = ~0ull;
-        c->far_epoch = vc->far_epoch + 1u;
-        c->r_epoch = vc->r_epoch + 1u;
-        c->in_count = vc->cnt[C_FAR0 + fin];
-        c->iterations = vc->iterations + 1u;
-        c->bucket_near = 0u;
-        c->bucket_rounds = 0u;
-        c->phase = PH_SCAN;
+        // keep the persistent stamp counters in step with the round descriptor
+        sc.near_epoch = r.near_epoch;
+        sc.far_epoch = r.far_epoch;
+        sc.r_epoch = r.r_epoch;
     }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
-// Bounded grid barrier. The last CTA to arrive runs `transition`, then opens
-// the barrier. A CTA that waits longer than p.timeout_ns, or sees an error
-// status, stops waiting and the kernel winds down; no wait is unbounded.
+// Bounded grid barrier with tickets: arrival k of the run belongs to barrier
+// (k-1)/G; the CTA holding the last ticket of a barrier loads the control
+// block into shared memory with parallel vector loads, runs `transition`,
+// stores it back and opens the barrier. A CTA that waits longer than
+// p.timeout_ns, or sees an error status, stops waiting and the kernel winds
+// down; no wait is unbounded.
 // ---------------------------------------------------------------------------
-__device__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, u32* s_flag,
+__device__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, Ctl& sc, u32* s_flag,
                              float* s_feat, float* act0, float* act1) {
     __syncthreads();
     Ctl* c = p.ctl;
@@ -590,58 +687,54 @@ __device__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, u3
     __shared__ u32 s_last, s_gen;
     if (threadIdx.x == 0) {
         if (fmin != ~0ull) atomicMin((unsigned long long*)&c->far_min[s.far_out], (unsigned long long)fmin);
-        const u32 gen = vload(&c->bar_gen);
         __threadfence();
-        const u32 arrived = atomicAdd(&c->bar_count, 1u) + 1u;
+        const u32 ticket = atomicAdd(&c->bar_count, 1u);
+        const u32 gen = ticket / gridDim.x;
         s_gen = gen;
-        s_last = arrived == gridDim.x ? 1u : 0u;
+        s_last = (ticket + 1u == (gen + 1u) * gridDim.x) ? 1u : 0u;
+        if (s_last) __threadfence();
     }
     __syncthreads();
+    constexpr u32 NCH = sizeof(Ctl) / 16;
     if (s_last) {
-        if (threadIdx.x == 0) {
-            c->bar_count = 0;
+        for (u32 i = threadIdx.x; i < NCH; i += blockDim.x)
+            reinterpret_cast<uint4*>(&sc)[i] = __ldcg(reinterpret_cast<const uint4*>(c) + i);
+        __syncthreads();
+        transition(p, sc, s_flag, s_feat, act0, act1);
+        for (u32 i = 1 + threadIdx.x; i < NCH; i += blockDim.x) {
+            __stcg(reinterpret_cast<uint4*>(c) + i, reinterpret_cast<const uint4*>(&sc)[i]);
             __threadfence();
         }
-        transition(p, s_flag, s_feat, act0, act1);
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
             atomicExch(&c->bar_gen, s_gen + 1u);
+            s = sc.rd;
         }
     } else if (threadIdx.x == 0) {
         const u64 t0 = global_timer_ns();
         u32 spins = 0;
-        while (vload(&c->bar_gen) == s_gen) {
-            __nanosleep(32);
-            if ((++spins & 63u) == 0u) {
-                if (vload(&c->status) != DS_OK) break;
+        bool ok = true;
+        while (vload(&c->bar_gen) <= s_gen) {
+            if ((++spins & 255u) == 0u) {
+                if (vload(&c->rd.status) != DS_OK) break;
                 if (global_timer_ns() - t0 > p.timeout_ns) {
-                    atomicCAS(&c->status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                    atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                    ok = false;
                     break;
                 }
+                if (spins > 4096u) __nanosleep(64);
             }
         }
-    }
-    if (threadIdx.x == 0) {
         __threadfence();
-        s.phase = vload(&c->phase);
-        s.in_count = vload(&c->in_count);
-        s.in_buf = vload(&c->in_buf);
-        s.far_in = vload(&c->far_in);
-        s.far_out = vload(&c->far_out);
-        s.status = vload(&c->status);
-        s.delta = vload(&c->delta);
-        s.heavy = vload(&c->heavy);
-        s.near_epoch = vload(&c->near_epoch);
-        s.far_epoch = vload(&c->far_epoch);
-        s.r_epoch = vload(&c->r_epoch);
-        s.naive_in = vload(&c->naive_in);
-        s.flag_epoch = vload(&c->flag_epoch);
-        s.map_mode = 1u;
-        s.lo = vload64(&c->lo);
-        s.hi = vload64(&c->hi);
-        if (s.status != DS_OK) s.phase = PH_DONE;
+        const uint4* src = reinterpret_cast<const uint4*>(&c->rd);
+        uint4* dst = reinterpret_cast<uint4*>(&s);
+        const uint4 a0 = __ldcg(src + 0), a1 = __ldcg(src + 1), a2 = __ldcg(src + 2),
+                    a3 = __ldcg(src + 3), a4 = __ldcg(src + 4);
+        dst[0] = a0; dst[1] = a1; dst[2] = a2; dst[3] = a3; dst[4] = a4;
+        if (!ok) s.status = DS_TIMEOUT;
     }
+    if (threadIdx.x == 0 && s.status != DS_OK) s.phase = PH_DONE;
     __syncthreads();
 }
 
@@ -652,6 +745,7 @@ template <bool ASTAR, int AM, int MAP>
 __global__ void __launch_bounds__(MAX_BS) k_persistent(const __grid_constant__ RunParams p) {
     __shared__ Snap s;
     __shared__ Coop cs;
+    __shared__ Ctl sc;
     __shared__ u64 red[32];
     __shared__ u32 s_flag[2];
     __shared__ float s_feat[POL_IN];
@@ -663,8 +757,11 @@ __global__ void __launch_bounds__(MAX_BS) k_persistent(const __grid_constant__ R
     const u64 gtid = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     const u64 gstride = (u64)gridDim.x * blockDim.x;
     for (u64 i = gtid; i < p.total; i += gstride) p.state[i] = STATE_INIT;
-    if (threadIdx.x == 0) s.far_out = 0;
-    grid_barrier(p, s, L, red, s_flag, s_feat, act0, act1);
+    if (threadIdx.x == 0) {
+        s.far_out = 0;
+        cs.cl_n = 0;
+    }
+    grid_barrier(p, s, L, red, sc, s_flag, s_feat, act0, act1);
 
     while (s.phase != PH_DONE) {
         const u32 ph = s.phase;
@@ -679,7 +776,7 @@ __global__ void __launch_bounds__(MAX_BS) k_persistent(const __grid_constant__ R
         } else if (ph == PH_COMPACT) {
             round_compact(p, s, cs);
         }
-        grid_barrier(p, s, L, red, s_flag, s_feat, act0, act1);
+        grid_barrier(p, s, L, red, sc, s_flag, s_feat, act0, act1);
     }
 
     // Per-warp reduction of the counters, one atomicAdd per warp.

@@ -374,6 +374,10 @@ static int env_int(const char* name, int dflt) {
     return atoi(v);
 }
 
+// Eager sub-rounds per grid round of the hybrid mapping when the caller leaves
+// the choice to the engine (pfg_options::eager < 0).
+static const int kDefaultEager = 4;
+
 static pfg_options default_options() {
     pfg_options o;
     o.algo = PFG_ALGO_DELTA;
@@ -384,6 +388,7 @@ static pfg_options default_options() {
     o.sync_every = 8;
     o.compaction = PFG_COMPACT_WARP_ATOMIC;
     o.policy = PFG_POLICY_FIXED;
+    o.eager = -1;
     return o;
 }
 
@@ -436,14 +441,15 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     Ctl* c = s->h_ctl;
     const size_t run_bytes = offsetof(Ctl, persist);
     memset(c, 0, run_bytes);
-    c->phase = PH_INIT;
-    c->far_out = 0;
+    c->rd.phase = PH_INIT;
+    c->rd.far_out = 0;
+    c->rd.map_mode = 1u;
     c->far_min[0] = c->far_min[1] = ~0ull;
     const u64 cap = 4ull * s->n + 1000ull;
     c->round_cap = (u32)std::min<u64>(cap, 0x7FFFFFFFull);
-    c->delta = delta ? delta : 1u;
+    c->rd.delta = delta ? delta : 1u;
     c->delta0 = delta;
-    c->heavy = (mode == MODE_DELTA && delta < s->maxw) ? 1u : 0u;
+    c->rd.heavy = (mode == MODE_DELTA && delta < s->maxw) ? 1u : 0u;
 
     RunParams p;
     memset(&p, 0, sizeof(p));
@@ -483,6 +489,7 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     p.mode = mode;
     p.prefix_scan = (mode == MODE_FRONTIER && o.compaction == PFG_COMPACT_PREFIX_SCAN) ? 1 : 0;
     p.policy = (mode == MODE_DELTA && o.policy == PFG_POLICY_LEARNED) ? 1 : 0;
+    p.eager = o.eager < 0 ? (u32)std::max(0, env_int("PFG_EAGER", kDefaultEager)) : (u32)o.eager;
     p.net = s->d_net;
     p.timeout_ns = (u64)std::max(1, env_int("PFG_TIMEOUT_MS", 2000)) * 1000000ull;
 
@@ -493,6 +500,9 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     const int cap_bps = env_int("PFG_BLOCKS_PER_SM", 0);
     if (cap_bps > 0) bps = std::min(bps, cap_bps);
     const int grid = s->sm_count * bps;
+    // Eager propagation pays in rounds that leave most of the GPU idle: inputs
+    // of at most a quarter of the launched threads.
+    p.eager_max_items = (u32)std::max<long long>(1, (long long)grid * block / 4);
 
     if (timed) PFG_CUDA(cudaEventRecord(s->ev0, s->stream));
     if (h_srcs) {
@@ -535,14 +545,15 @@ static pfg_status complete_run(pfg_solver* s, pfg_stats* stats_out) {
         stats_out->delta = s->last_delta;
         stats_out->rounds = c->rounds;
     }
-    if (c->status == DS_TIMEOUT) {
+    const u32 status = c->rd.status;
+    if (status == DS_TIMEOUT) {
         // A wait gave up: reset the naive masks so the next run starts clean.
         const u64 words = (u64)s->n / 32 + 1;
         for (int i = 0; i < 2; ++i) cudaMemsetAsync(s->d_naive[i], 0, words * 4, s->stream);
         cudaStreamSynchronize(s->stream);
         return fail(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
     }
-    if (c->status == DS_NOT_CONVERGED) {
+    if (status == DS_NOT_CONVERGED) {
         const u64 words = (u64)s->n / 32 + 1;
         for (int i = 0; i < 2; ++i) cudaMemsetAsync(s->d_naive[i], 0, words * 4, s->stream);
         cudaStreamSynchronize(s->stream);
@@ -550,8 +561,8 @@ static pfg_status complete_run(pfg_solver* s, pfg_stats* stats_out) {
                          : s->last_mode == MODE_FRONTIER ? "Frontier relaxation" : "Delta-stepping";
         return fail(PFG_ERR_NOT_CONVERGED, "%s did not converge", what);
     }
-    if (c->status == DS_BAD_SOURCE) return fail(PFG_ERR_INVALID_ARGUMENT, "source out of range");
-    if (c->status != DS_OK) return fail(PFG_ERR_CUDA, "device status %u", c->status);
+    if (status == DS_BAD_SOURCE) return fail(PFG_ERR_INVALID_ARGUMENT, "source out of range");
+    if (status != DS_OK) return fail(PFG_ERR_CUDA, "device status %u", status);
     return PFG_OK;
 }
 

@@ -61,11 +61,12 @@ class GpuOptions:
     syncEvery: int = 8
     compaction: Compaction = Compaction.WarpAtomic
     policy: Policy = Policy.Fixed
+    eager: int = -1  # Hybrid mapping: eager sub-rounds per grid round (-1 engine default, 0 off)
 
     def to_c(self) -> N.PfgOptions:
         return N.PfgOptions(int(self.algo), int(self.mapping), int(self.atomic), int(self.delta),
                             int(self.blockSize), int(self.syncEvery), int(self.compaction),
-                            int(self.policy))
+                            int(self.policy), int(self.eager))
 
 
 @dataclass

@@ -80,6 +80,22 @@ def test_grid100_delta_sweep(oracle, grid100, grid100_solver, delta):
     assert res.stats.delta == delta
 
 
+@pytest.mark.parametrize("eager", [0, 1, 3, 16, 64])
+def test_grid100_eager_subrounds(oracle, grid100, grid100_solver, eager):
+    # in-round propagation changes the schedule only: results stay bit-exact
+    for algo in (GpuAlgo.DeltaStep, GpuAlgo.Frontier):
+        for src in (0, 5050, 9999):
+            res = grid100_solver.sssp(src, GpuOptions(algo=algo, eager=eager))
+            check_sssp(oracle, grid100, src, res)
+
+
+def test_rmat_eager_subrounds(oracle, rmat12, rmat12_solver):
+    s = int(pf.pick_sources(rmat12, 1, 11)[0])
+    for eager in (0, 2, 32):
+        for delta in (0, 8):
+            check_sssp(oracle, rmat12, s, rmat12_solver.sssp(s, GpuOptions(eager=eager, delta=delta)))
+
+
 def test_grid100_prefix_scan(oracle, grid100, grid100_solver):
     res = grid100_solver.sssp(5, GpuOptions(algo=GpuAlgo.Frontier, compaction=Compaction.PrefixScan))
     check_sssp(oracle, grid100, 5, res)
