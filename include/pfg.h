@@ -198,6 +198,35 @@ PFG_API pfg_status pfg_transfer_study_run(const uint32_t* row_offsets, const uin
 PFG_API pfg_status pfg_set_policy(pfg_solver* s, const float* params, uint64_t count);
 PFG_API uint64_t pfg_policy_param_count(void);
 
+/* ---- SSSP without any allocation (no counterpart in the reference) ----
+ * For callers that may not allocate device memory themselves or through
+ * this library: code inside a host application or framework that owns all
+ * device memory through its own pool and hands a plugin only the buffers it
+ * may use, or a latency-critical loop that cannot afford cudaMalloc's
+ * implicit synchronisation. Runs the persistent Delta-stepping kernel of
+ * pfg_run (Hybrid mapping, MinRBA atomics, fixed `delta` >= 1) from `src`
+ * on a CSR already in device memory (rows sorted by weight, weights >= 1),
+ * writing n packed (dist << 32 | parent) words to d_state_out and
+ * [status, rounds, buckets, non-empty rounds] to d_status_out[0..3]
+ * (status is a pfg_status value). Work is enqueued on `stream` (a
+ * cudaStream_t of the current device) and the call returns without waiting;
+ * read d_status_out after synchronising.
+ * All scratch lives in one fixed device array compiled into the library
+ * (about 7.6 MB, held by every device the library's module is loaded on
+ * until the process exits), so the graph is limited to n <=
+ * PFG_NOALLOC_MAX_VERTICES and m + 3n <= PFG_NOALLOC_MAX_ARCS; larger inputs
+ * return PFG_ERR_CAPACITY before anything is launched. The first call on a
+ * device looks up the array's device address (this also loads the module on
+ * that device); make that first call before any stream capture. Every call
+ * on a device shares the one array, so calls that overlap on the GPU (two
+ * streams, two threads) race and corrupt each other: serialise them. */
+#define PFG_NOALLOC_MAX_VERTICES 65536u
+#define PFG_NOALLOC_MAX_ARCS 655360u
+PFG_API pfg_status pfg_sssp_noalloc(const uint32_t* d_row_offsets, const uint32_t* d_col_indices,
+                                    const uint32_t* d_weights, uint32_t n, uint32_t m, uint32_t src,
+                                    uint32_t delta, uint64_t* d_state_out, uint32_t* d_status_out,
+                                    void* stream);
+
 /* ---- errors ---- */
 PFG_API const char* pfg_last_error(void);
 PFG_API const char* pfg_status_string(pfg_status st);

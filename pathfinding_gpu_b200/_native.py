@@ -77,6 +77,8 @@ SIGNATURES = {
     "pfg_transfer_study_run": (i32, [P(u32), P(u32), P(u32), u32, u32, i32, P(PfgTransferStudy)]),
     "pfg_set_policy": (i32, [C.c_void_p, P(f32), u64]),
     "pfg_policy_param_count": (u64, []),
+    "pfg_sssp_noalloc": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32, u32, u32, u32, C.c_void_p,
+                               C.c_void_p, C.c_void_p]),
     "pfg_last_error": (C.c_char_p, []),
     "pfg_status_string": (C.c_char_p, [i32]),
     "pfg_abi_version": (i32, []),
