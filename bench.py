@@ -54,43 +54,10 @@ def parse():
 # ---------------------------------------------------------------------------
 # distributed plumbing (one process per GPU, torchrun env)
 # ---------------------------------------------------------------------------
-class Dist:
-    def __init__(self, n):
-        import torch
-        self.torch = torch
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
-        if self.world > 1:
-            import torch.distributed as dist
-            from datetime import timedelta
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local))
-            self.pg = dist
-
-    def barrier(self):
-        if self.pg:
-            self.pg.barrier()
-
-    def max(self, x: float) -> float:
-        if not self.pg:
-            return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum(self, x: float) -> float:
-        if not self.pg:
-            return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
-        return float(t.item())
-
-    def close(self):
-        if self.pg:
-            self.pg.destroy_process_group()
+def Dist(n_gpus: int):
+    """Replica process group (NCCL), one process per GPU; see pathfinding_gpu_b200/replicas.py."""
+    from pathfinding_gpu_b200.replicas import ReplicaGroup
+    return ReplicaGroup(backend="nccl" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else None)
 
 
 # ---------------------------------------------------------------------------
@@ -190,7 +157,7 @@ def reachable_stats(g, dist_rows):
 # ---------------------------------------------------------------------------
 # our implementation
 # ---------------------------------------------------------------------------
-def run_ours(args, D: "Dist"):
+def run_ours(args, D):
     import torch
     import pathfinding_gpu_b200 as pf
     from pathfinding_gpu_b200 import GpuOptions
@@ -350,7 +317,7 @@ def extras(g):
     return out
 
 
-def run_reference(args, D: "Dist"):
+def run_reference(args, D):
     if D.rank != 0:
         return None
     import pathfinding_gpu_b200 as pf
