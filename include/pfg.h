@@ -75,6 +75,8 @@ typedef struct pfg_options {
     int32_t policy;      /* enum pfg_policy_kind (Delta-stepping only)            */
     int32_t eager;       /* Hybrid mapping: in-round propagation sub-rounds per
                             grid round; -1 = engine default, 0 = off (extension) */
+    int32_t blocks_per_sm; /* CTAs of the persistent kernel per SM; 0 = engine
+                              default (1024 resident threads per SM) (extension) */
 } pfg_options;
 
 /* Mirrors GpuStats (reference: include/gpu_sssp.h:55-65) plus `rounds`. */
@@ -186,6 +188,41 @@ typedef struct pfg_transfer_study {
 PFG_API pfg_status pfg_transfer_study_run(const uint32_t* row_offsets, const uint32_t* col_indices,
                                   const uint32_t* weights, uint32_t n, uint32_t m,
                                   int32_t reps, pfg_transfer_study* out);
+
+/* ---- batches of uneven instances (extension of multiSource) ----
+ * The reference's multiSource batches K sources of one graph with state
+ * index k*n + v (src/gpu_kernels.cuh:223-225). A batch generalises this to
+ * per-instance offsets: it holds num_graphs CSR graphs (rows sorted by
+ * weight) and a table of instances (graph, source); instance i owns the
+ * packed state words [pfg_batch_instance_offset(i), ...(i+1)). One
+ * persistent launch relaxes every instance with one shared bucket
+ * sequence; per-instance results equal single-source runs bit for bit.
+ * max_states bounds the sum of the instances' vertex counts (< 2^32). */
+typedef struct pfg_batch pfg_batch;
+PFG_API pfg_status pfg_batch_create(uint32_t num_graphs, const uint32_t* const* row_offsets,
+                                    const uint32_t* const* col_indices,
+                                    const uint32_t* const* weights, const uint32_t* n,
+                                    const uint32_t* m, uint64_t max_states,
+                                    uint32_t max_instances, int32_t device, pfg_batch** out);
+PFG_API void pfg_batch_destroy(pfg_batch* b);
+/* Instance i = (inst_graph[i], inst_src[i]). Replaces any recorded run. */
+PFG_API pfg_status pfg_batch_set_instances(pfg_batch* b, const uint32_t* inst_graph,
+                                           const uint32_t* inst_src, uint32_t count);
+/* One launch over all instances; ms_out = device time (CUDA events). */
+PFG_API pfg_status pfg_batch_run(pfg_batch* b, const pfg_options* opt, pfg_stats* stats_out,
+                                 float* ms_out);
+/* Records one run (control-block upload, persistent launch, read-back) into a
+ * CUDA graph; pfg_batch_replay launches it again with the same options and
+ * instances and returns its statistics. */
+PFG_API pfg_status pfg_batch_capture(pfg_batch* b, const pfg_options* opt);
+PFG_API pfg_status pfg_batch_replay(pfg_batch* b, pfg_stats* stats_out, float* ms_out);
+PFG_API uint64_t pfg_batch_instance_offset(const pfg_batch* b, uint32_t inst);
+PFG_API uint64_t pfg_batch_num_states(const pfg_batch* b);
+PFG_API pfg_status pfg_batch_copy_state(pfg_batch* b, uint64_t first, uint64_t count,
+                                        uint64_t* h_out);
+PFG_API void* pfg_batch_stream(const pfg_batch* b);
+PFG_API double pfg_batch_upload_ms(const pfg_batch* b);
+PFG_API uint64_t pfg_batch_device_bytes(const pfg_batch* b);
 
 /* ---- learned Delta policy (extension; no reference counterpart) ----
  * The policy is a 12 -> 64 -> 64 -> 64 -> 8 fp32 MLP evaluated on the device

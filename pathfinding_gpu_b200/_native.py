@@ -26,7 +26,7 @@ STATUS_NAMES = {
 class PfgOptions(C.Structure):
     _fields_ = [("algo", i32), ("mapping", i32), ("atomic", i32), ("delta", u32),
                 ("block_size", i32), ("sync_every", u32), ("compaction", i32), ("policy", i32),
-                ("eager", i32)]
+                ("eager", i32), ("blocks_per_sm", i32)]
 
 
 class PfgStats(C.Structure):
@@ -77,6 +77,19 @@ SIGNATURES = {
     "pfg_transfer_study_run": (i32, [P(u32), P(u32), P(u32), u32, u32, i32, P(PfgTransferStudy)]),
     "pfg_set_policy": (i32, [C.c_void_p, P(f32), u64]),
     "pfg_policy_param_count": (u64, []),
+    "pfg_batch_create": (i32, [u32, P(P(u32)), P(P(u32)), P(P(u32)), P(u32), P(u32), u64, u32, i32,
+                               P(C.c_void_p)]),
+    "pfg_batch_destroy": (None, [C.c_void_p]),
+    "pfg_batch_set_instances": (i32, [C.c_void_p, P(u32), P(u32), u32]),
+    "pfg_batch_run": (i32, [C.c_void_p, P(PfgOptions), P(PfgStats), P(f32)]),
+    "pfg_batch_capture": (i32, [C.c_void_p, P(PfgOptions)]),
+    "pfg_batch_replay": (i32, [C.c_void_p, P(PfgStats), P(f32)]),
+    "pfg_batch_instance_offset": (u64, [C.c_void_p, u32]),
+    "pfg_batch_num_states": (u64, [C.c_void_p]),
+    "pfg_batch_copy_state": (i32, [C.c_void_p, u64, u64, P(u64)]),
+    "pfg_batch_stream": (C.c_void_p, [C.c_void_p]),
+    "pfg_batch_upload_ms": (f64, [C.c_void_p]),
+    "pfg_batch_device_bytes": (u64, [C.c_void_p]),
     "pfg_sssp_noalloc": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32, u32, u32, u32, C.c_void_p,
                                C.c_void_p, C.c_void_p]),
     "pfg_last_error": (C.c_char_p, []),

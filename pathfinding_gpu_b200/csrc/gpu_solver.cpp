@@ -30,6 +30,7 @@ pfg_options to_c(const GpuOptions& o) {
     c.compaction = static_cast<int32_t>(o.compaction);
     c.policy = PFG_POLICY_FIXED;
     c.eager = -1;
+    c.blocks_per_sm = 0;
     return c;
 }
 

@@ -139,6 +139,11 @@ struct RunParams {
     int mode;          // RunMode
     int prefix_scan;   // 1: flag + scan compaction instead of queue pushes
     int policy;        // 1: learned Delta policy picks each bucket's Delta
+    // Uneven instances (batch API): instance i owns state words
+    // [inst_off[i], inst_off[i+1]) and its graph's padded row starts begin at
+    // prow[inst_rowbase[i]]. nullptr: uniform instances of one graph, i*n + v.
+    const u32* inst_off;
+    const u32* inst_rowbase;
     u32 eager;         // hybrid mapping: eager sub-rounds per round (0 = off)
     u32 eager_max_items;  // ... only in rounds whose input has at most this many items
     const PolicyNet* net;

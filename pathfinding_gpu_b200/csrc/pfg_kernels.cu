@@ -197,8 +197,20 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
                                           Local& L, u32& u, u32& ib, u32& du, u32& ub, u32& eb,
                                           u32& ee) {
     Ctl* c = p.ctl;
-    const u32 inst = p.k > 1 ? gi / p.n : 0u;
-    ib = inst * p.n;
+    u32 rb = 0;  // first padded row start of the item's graph
+    if (p.inst_off) {
+        // uneven instances: last instance whose offset is <= gi
+        u32 lo = 0, hi = p.k - 1;
+        while (lo < hi) {
+            const u32 mid = (lo + hi + 1) >> 1;
+            if (__ldg(p.inst_off + mid) <= gi) lo = mid; else hi = mid - 1;
+        }
+        ib = __ldg(p.inst_off + lo);
+        rb = __ldg(p.inst_rowbase + lo);
+    } else {
+        const u32 inst = p.k > 1 ? gi / p.n : 0u;
+        ib = inst * p.n;
+    }
     u = gi - ib;
     du = st_dist(ld_state(p.state + gi));
     bool act = du != INF32;
@@ -223,7 +235,7 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
         }
     }
     if (!act) return false;
-    const u32 r0 = __ldg(p.prow + u), r1 = __ldg(p.prow + u + 1);
+    const u32 r0 = __ldg(p.prow + rb + u), r1 = __ldg(p.prow + rb + u + 1);
     if (kind == K_HEAVY) {
         eb = light_end(p.adj, r0, r1, s.delta);
         ee = r1;
@@ -510,9 +522,12 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
             r.r_epoch = sc.r_epoch + 1u;
             // Seed the k sources (reference seedKernel, src/gpu_kernels.cuh:340-352).
             bool bad = false;
-            for (u32 i = 0; i < p.k; ++i) bad = bad || p.srcs[i] >= p.n;
+            for (u32 i = 0; i < p.k; ++i) {
+                const u32 ni = p.inst_off ? p.inst_off[i + 1] - p.inst_off[i] : p.n;
+                bad = bad || p.srcs[i] >= ni;
+            }
             for (u32 i = 0; i < p.k && !bad; ++i) {
-                const u32 gi = i * p.n + p.srcs[i];
+                const u32 gi = (p.inst_off ? p.inst_off[i] : i * p.n) + p.srcs[i];
                 p.state[gi] = pack_state(0u, NO_PARENT);
                 if (p.mode != MODE_NAIVE) p.nearq[0][i] = gi;
             }
@@ -829,9 +844,20 @@ static const void* kernel_for(bool astar, int am, int map) {
 
 cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, int block,
                               int grid, cudaStream_t st) {
+    // Cooperative attribute: the driver refuses a grid that cannot be fully
+    // resident, which the grid barrier relies on. Also valid in stream capture.
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     void* args[] = {(void*)&p};
-    return cudaLaunchCooperativeKernel(kernel_for(astar, am, map), dim3(grid), dim3(block), args,
-                                       0, st);
+    return cudaLaunchKernelExC(&cfg, kernel_for(astar, am, map), args);
 }
 
 int persistent_blocks_per_sm(bool astar, int am, int map, int block) {

@@ -7,6 +7,7 @@
 #include "../../include/pfg.h"
 #include "pfg_common.cuh"
 #include "pfg_kernels.h"
+#include "pfg_internal.h"
 
 #include <algorithm>
 #include <chrono>
@@ -26,6 +27,16 @@ using namespace pfg;
 static thread_local std::string g_last_error;
 
 static pfg_status fail(pfg_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+pfg_status pfg::set_error(pfg_status st, const char* fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -125,7 +136,7 @@ struct pfg_solver {
     }
 };
 
-static u32 auto_delta_of(double avg_w, double avg_deg) {
+u32 pfg::auto_delta_of(double avg_w, double avg_deg) {
     // Davidson et al.: Delta ~ warp size * average weight / average degree
     // (reference: src/gpu_sssp.cu:202-206).
     const double d = 32.0 * avg_w / std::max(1.0, avg_deg);
@@ -147,7 +158,7 @@ static void destroy_solver(pfg_solver* s) {
     delete s;
 }
 
-static pfg_status validate_csr(const uint32_t* row, const uint32_t* col, const uint32_t* w,
+pfg_status pfg::validate_csr(const uint32_t* row, const uint32_t* col, const uint32_t* w,
                                uint32_t n, uint32_t m, u32* maxw_out) {
     if (n == 0) return fail(PFG_ERR_INVALID_GRAPH, "graph has no vertices");
     if (!row || (m > 0 && (!col || !w)))
@@ -378,7 +389,9 @@ static int env_int(const char* name, int dflt) {
 // the choice to the engine (pfg_options::eager < 0).
 static const int kDefaultEager = 4;
 
-static pfg_options default_options() {
+namespace pfg {
+
+pfg_options default_options() {
     pfg_options o;
     o.algo = PFG_ALGO_DELTA;
     o.mapping = PFG_MAP_HYBRID;
@@ -389,8 +402,35 @@ static pfg_options default_options() {
     o.compaction = PFG_COMPACT_WARP_ATOMIC;
     o.policy = PFG_POLICY_FIXED;
     o.eager = -1;
+    o.blocks_per_sm = 0;
     return o;
 }
+
+void sanitize_options(pfg_options& o) {
+    // Silent fix-up of the reference (src/gpu_sssp.cu:462).
+    if (o.block_size < 32 || o.block_size > 1024 || (o.block_size % 32) != 0) o.block_size = 256;
+    if (o.mapping < 0 || o.mapping > 2) o.mapping = PFG_MAP_HYBRID;
+    if (o.atomic < 0 || o.atomic > 2) o.atomic = PFG_ATOMIC_MIN_RBA;
+}
+
+int blocks_per_sm_for(const pfg_options& o, bool astar, int map) {
+    int bps = persistent_blocks_per_sm(astar, o.atomic, map, o.block_size);
+    if (bps <= 0) return 0;
+    // Default: fill each SM up to 1024 resident threads (more CTAs only make
+    // the grid barrier slower on this latency-bound kernel).
+    int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : std::max(1, 1024 / o.block_size);
+    const int cap = env_int("PFG_BLOCKS_PER_SM", 0);
+    if (cap > 0) want = cap;
+    return std::max(1, std::min(bps, want));
+}
+
+u32 eager_rounds_for(const pfg_options& o) {
+    return o.eager < 0 ? (u32)std::max(0, env_int("PFG_EAGER", kDefaultEager)) : (u32)o.eager;
+}
+
+u64 device_timeout_ns() { return (u64)std::max(1, env_int("PFG_TIMEOUT_MS", 2000)) * 1000000ull; }
+
+}  // namespace pfg
 
 // Resets the stamp words when the epoch counters approach 2^32.
 static pfg_status maybe_reset_epochs(pfg_solver* s) {
@@ -414,8 +454,7 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
                               bool timed) {
     if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
     pfg_options o = opt_in ? *opt_in : default_options();
-    // Silent fix-ups of the reference (src/gpu_sssp.cu:462,466).
-    if (o.block_size < 32 || o.block_size > 1024 || (o.block_size % 32) != 0) o.block_size = 256;
+    sanitize_options(o);
     if (k == 0 || k > s->K) return fail(PFG_ERR_INVALID_ARGUMENT, "invalid batch size");
     if (h_srcs) {
         for (u32 i = 0; i < k; ++i)
@@ -489,16 +528,14 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     p.mode = mode;
     p.prefix_scan = (mode == MODE_FRONTIER && o.compaction == PFG_COMPACT_PREFIX_SCAN) ? 1 : 0;
     p.policy = (mode == MODE_DELTA && o.policy == PFG_POLICY_LEARNED) ? 1 : 0;
-    p.eager = o.eager < 0 ? (u32)std::max(0, env_int("PFG_EAGER", kDefaultEager)) : (u32)o.eager;
+    p.eager = eager_rounds_for(o);
     p.net = s->d_net;
-    p.timeout_ns = (u64)std::max(1, env_int("PFG_TIMEOUT_MS", 2000)) * 1000000ull;
+    p.timeout_ns = device_timeout_ns();
 
     const int map = mode == MODE_NAIVE ? PFG_MAP_THREAD : o.mapping;
     const int block = o.block_size;
-    int bps = persistent_blocks_per_sm(astar != 0, o.atomic, map, block);
+    const int bps = blocks_per_sm_for(o, astar != 0, map);
     if (bps <= 0) return fail(PFG_ERR_CUDA, "occupancy query failed for block size %d", block);
-    const int cap_bps = env_int("PFG_BLOCKS_PER_SM", 0);
-    if (cap_bps > 0) bps = std::min(bps, cap_bps);
     const int grid = s->sm_count * bps;
     // Eager propagation pays in rounds that leave most of the GPU idle: inputs
     // of at most a quarter of the launched threads.

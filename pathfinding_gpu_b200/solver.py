@@ -62,11 +62,12 @@ class GpuOptions:
     compaction: Compaction = Compaction.WarpAtomic
     policy: Policy = Policy.Fixed
     eager: int = -1  # Hybrid mapping: eager sub-rounds per grid round (-1 engine default, 0 off)
+    blocksPerSM: int = 0  # CTAs of the persistent kernel per SM (0: engine default)
 
     def to_c(self) -> N.PfgOptions:
         return N.PfgOptions(int(self.algo), int(self.mapping), int(self.atomic), int(self.delta),
                             int(self.blockSize), int(self.syncEvery), int(self.compaction),
-                            int(self.policy), int(self.eager))
+                            int(self.policy), int(self.eager), int(self.blocksPerSM))
 
 
 @dataclass
