@@ -234,6 +234,27 @@ PFG_API uint64_t pfg_batch_device_bytes(const pfg_batch* b);
  * in_mean[12] in_scale[12]). */
 PFG_API pfg_status pfg_set_policy(pfg_solver* s, const float* params, uint64_t count);
 PFG_API uint64_t pfg_policy_param_count(void);
+/* A Delta-stepping run (fixed or learned Delta) that also returns, for every
+ * bucket advance, one trace row of 16 floats: the 12 policy features, then
+ * the bucket index, the Delta of the bucket that ended, the items that entered
+ * it and the rounds it took. *rows_out = rows written (<= trace_cap). */
+PFG_API pfg_status pfg_run_traced(pfg_solver* s, const uint32_t* h_srcs, uint32_t k,
+                                  const pfg_options* opt, pfg_stats* stats_out, float* h_trace,
+                                  uint32_t trace_cap, uint32_t* rows_out, float* ms_out);
+/* Training and inference of the policy network on the GPU (hand-written
+ * kernels). Samples are rows of 12 features (h_x, n x 12) with soft targets
+ * over the 8 Delta classes (h_y, n x 8, each row summing to 1); the loss is
+ * the mean cross-entropy. pfg_policy_grad returns the loss and its gradient
+ * for every parameter (zero for the fixed input normalisation);
+ * pfg_policy_train runs `steps` full-batch Adam steps in place and writes the
+ * loss of each step to loss_out (nullable); pfg_policy_infer returns the
+ * argmax class per sample. */
+PFG_API pfg_status pfg_policy_grad(const float* h_params, const float* h_x, const float* h_y,
+                                   uint32_t n, float* h_grad_out, float* loss_out);
+PFG_API pfg_status pfg_policy_train(float* h_params, const float* h_x, const float* h_y,
+                                    uint32_t n, uint32_t steps, float lr, float* loss_out);
+PFG_API pfg_status pfg_policy_infer(const float* h_params, const float* h_x, uint32_t n,
+                                    uint32_t* h_class_out);
 
 /* ---- SSSP without any allocation (no counterpart in the reference) ----
  * For callers that may not allocate device memory themselves or through

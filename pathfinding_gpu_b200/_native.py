@@ -77,6 +77,11 @@ SIGNATURES = {
     "pfg_transfer_study_run": (i32, [P(u32), P(u32), P(u32), u32, u32, i32, P(PfgTransferStudy)]),
     "pfg_set_policy": (i32, [C.c_void_p, P(f32), u64]),
     "pfg_policy_param_count": (u64, []),
+    "pfg_run_traced": (i32, [C.c_void_p, P(u32), u32, P(PfgOptions), P(PfgStats), P(f32), u32, P(u32),
+                             P(f32)]),
+    "pfg_policy_grad": (i32, [P(f32), P(f32), P(f32), u32, P(f32), P(f32)]),
+    "pfg_policy_train": (i32, [P(f32), P(f32), P(f32), u32, u32, f32, P(f32)]),
+    "pfg_policy_infer": (i32, [P(f32), P(f32), u32, P(u32)]),
     "pfg_batch_create": (i32, [u32, P(P(u32)), P(P(u32)), P(P(u32)), P(u32), P(u32), u64, u32, i32,
                                P(C.c_void_p)]),
     "pfg_batch_destroy": (None, [C.c_void_p]),

@@ -100,6 +100,7 @@ static_assert(sizeof(Rd) == 80, "Rd layout");
 constexpr int POL_IN = 12;
 constexpr int POL_H = 64;
 constexpr int POL_OUT = 8;  // Delta multipliers, see kPolicyMult
+constexpr int TRACE_W = 16; // trace row: POL_IN features, then bucket index, Delta, items, rounds
 struct PolicyNet {
     float w1[POL_H * POL_IN], b1[POL_H];
     float w2[POL_H * POL_H], b2[POL_H];
@@ -139,6 +140,8 @@ struct RunParams {
     int mode;          // RunMode
     int prefix_scan;   // 1: flag + scan compaction instead of queue pushes
     int policy;        // 1: learned Delta policy picks each bucket's Delta
+    float* trace;      // optional: TRACE_W floats per bucket advance (policy features)
+    u32 trace_cap;     // rows available in trace
     // Uneven instances (batch API): instance i owns state words
     // [inst_off[i], inst_off[i+1]) and its graph's padded row starts begin at
     // prow[inst_rowbase[i]]. nullptr: uniform instances of one graph, i*n + v.

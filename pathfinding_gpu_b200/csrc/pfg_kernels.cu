@@ -41,6 +41,7 @@ typedef Rd Snap;
 
 struct Local {
     u32 edges = 0, atomics = 0, updates = 0, pushes = 0;
+    u32 edges_flushed = 0;  // value of `edges` at the last per-round flush (policy / trace)
     u64 fmin = ~0ull;  // smallest key this thread pushed to the far pile this round
 };
 
@@ -494,9 +495,46 @@ __device__ u32 policy_pick(const PolicyNet* net, const float* feat, float* act0,
 // the logic, the whole CTA evaluates the policy network when a bucket advance
 // asks for it).
 // ---------------------------------------------------------------------------
+// Features of a decision point (the start of the first bucket, or a bucket
+// advance), computed by thread 0 of the transition CTA:
+//   0 log2(1 + items of the next bucket's input)   6 log2(Delta / avgW)
+//   1 log2(1 + items that entered the last bucket) 7 log2(1 + avgDeg)
+//   2 log2(1 + rounds of the last bucket)          8 log2(maxW / avgW)
+//   3 (next smallest key - window end) / avgW      9 log2(1 + n)
+//   4 log2(1 + arcs scanned in the last bucket)   10 next smallest key / (avgW sqrt(n))
+//   5 log2(1 + buckets so far)                    11 min(1, Delta / maxW)
+// With tracing on, the row is also written to p.trace (decision k -> row k).
+__device__ void decision_features(const RunParams& p, Ctl& sc, const Rd& r, u32 fn, u64 est, float* f) {
+    const double aw = p.avg_w > 0.0 ? p.avg_w : 1.0;
+    const u64 edges_now = sc.bucket_edges_acc;
+    f[0] = log2f(1.f + (float)fn);
+    f[1] = log2f(1.f + (float)sc.bucket_near);
+    f[2] = log2f(1.f + (float)sc.bucket_rounds);
+    f[3] = (float)((double)(est > r.hi ? est - r.hi : 0ull) / aw);
+    f[4] = log2f(1.f + (float)(edges_now - sc.bucket_edges));
+    f[5] = log2f(1.f + (float)sc.buckets);
+    f[6] = log2f((float)((double)r.delta / aw));
+    f[7] = log2f(1.f + (float)p.avg_deg);
+    f[8] = log2f((float)((double)p.maxw / aw));
+    f[9] = log2f(1.f + (float)p.n);
+    f[10] = (float)((double)est / (aw * sqrt((double)p.n)));
+    f[11] = fminf(1.f, (float)r.delta / (float)(p.maxw ? p.maxw : 1u));
+    sc.bucket_edges = edges_now;
+    const u32 row = sc.buckets;
+    if (p.trace && row < p.trace_cap) {
+        float* tr = p.trace + (size_t)row * TRACE_W;
+        for (int i = 0; i < POL_IN; ++i) tr[i] = f[i];
+        tr[POL_IN + 0] = (float)sc.buckets;
+        tr[POL_IN + 1] = (float)r.delta;
+        tr[POL_IN + 2] = (float)sc.bucket_near;
+        tr[POL_IN + 3] = (float)sc.bucket_rounds;
+    }
+}
+
 __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_feat, float* act0,
                            float* act1) {
     const u32 t = threadIdx.x;
+    __shared__ u64 s_key0;
     // s_flag[0]: 0 = no bucket advance, 1 = advance with the policy, 2 = fixed Delta
     if (t == 0) {
         Rd& r = sc.rd;
@@ -556,6 +594,15 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
                 sc.bucket_near = p.k;
                 sc.bucket_rounds = 0u;
                 r.phase = PH_LIGHT;
+                if (p.mode == MODE_DELTA && (p.policy || p.trace)) {
+                    // The first bucket is a decision point too: features of the
+                    // seed window (nothing relaxed yet) and the graph.
+                    decision_features(p, sc, r, p.k, key0, s_feat);
+                    if (p.policy) {
+                        s_flag[0] = 3u;  // choose the first bucket's Delta below
+                        s_key0 = key0;
+                    }
+                }
             }
         } else if (ph == PH_NAIVE) {
             sc.iterations += 1u;
@@ -621,36 +668,28 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
                 r.phase = PH_DONE;
             } else {
                 s_flag[0] = p.policy ? 1u : 2u;
-                if (p.policy) {
-                    const double aw = p.avg_w > 0.0 ? p.avg_w : 1.0;
-                    const u64 edges_now = sc.bucket_edges_acc;
-                    s_feat[0] = log2f(1.f + (float)fn);
-                    s_feat[1] = log2f(1.f + (float)sc.bucket_near);
-                    s_feat[2] = log2f(1.f + (float)sc.bucket_rounds);
-                    s_feat[3] = (float)((double)(est - r.hi) / aw);
-                    s_feat[4] = log2f(1.f + (float)(edges_now - sc.bucket_edges));
-                    s_feat[5] = log2f(1.f + (float)sc.buckets);
-                    s_feat[6] = log2f((float)((double)r.delta / aw));
-                    s_feat[7] = log2f(1.f + (float)p.avg_deg);
-                    s_feat[8] = log2f((float)((double)p.maxw / aw));
-                    s_feat[9] = log2f(1.f + (float)p.n);
-                    s_feat[10] = (float)((double)est / (aw * sqrt((double)p.n)));
-                    s_feat[11] = fminf(1.f, (float)r.delta / (float)(p.maxw ? p.maxw : 1u));
-                    sc.bucket_edges = edges_now;
-                }
+                if (p.policy || p.trace) decision_features(p, sc, r, fn, est, s_feat);
             }
         }
     }
     __syncthreads();
     const u32 need = s_flag[0];
-    if (need == 1u) {
+    if (need == 1u || need == 3u) {
         const u32 cls = policy_pick(p.net, s_feat, act0, act1);
         if (t == 0) s_flag[1] = cls;
     }
     __syncthreads();
     if (t == 0) {
         Rd& r = sc.rd;
-        if (need != 0u) {
+        if (need == 3u) {
+            // first bucket under the policy: window [key0, key0 + Delta)
+            const float dm = (float)p.delta * kPolicyMult[s_flag[1]];
+            const u32 d = dm < 1.f ? 1u : (dm > 2.0e9f ? 2000000000u : (u32)dm);
+            r.delta = d;
+            r.heavy = d < p.maxw ? 1u : 0u;
+            r.hi = s_key0 + d;
+            sc.policy_calls += 1u;
+        } else if (need != 0u) {
             // Open the next bucket: the far pile collected during this bucket is
             // scanned against the window [old hi, new hi).
             u32 d = p.delta;
@@ -700,6 +739,16 @@ __device__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, Ct
     const u64 fmin = block_min_u64(L.fmin, red);
     L.fmin = ~0ull;
     __shared__ u32 s_last, s_gen;
+    if (p.policy || p.trace) {
+        // Arcs scanned this round (for the policy's per-bucket work feature):
+        // each thread's count since the last flush, one atomicAdd per warp.
+        u32 x = L.edges - L.edges_flushed;
+        L.edges_flushed = L.edges;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(FULL, x, o);
+        if ((threadIdx.x & 31u) == 0 && x)
+            atomicAdd((unsigned long long*)&c->bucket_edges_acc, (unsigned long long)x);
+    }
     if (threadIdx.x == 0) {
         if (fmin != ~0ull) atomicMin((unsigned long long*)&c->far_min[s.far_out], (unsigned long long)fmin);
         __threadfence();

@@ -106,6 +106,8 @@ struct pfg_solver {
     Ctl* d_ctl = nullptr;
     PolicyNet* d_net = nullptr;
     bool has_net = false;
+    float* d_trace = nullptr;   // per-bucket policy features of traced runs
+    u32 trace_cap = 0;
 
     Ctl* h_ctl = nullptr;       // pinned mirror of the control block
     u32* h_srcs = nullptr;      // pinned staging of the sources [K]
@@ -151,6 +153,7 @@ static void destroy_solver(pfg_solver* s) {
     for (void* p : s->allocs) cudaFree(p);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->h_srcs) cudaFreeHost(s->h_srcs);
+    if (s->d_trace) cudaFree(s->d_trace);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -451,7 +454,7 @@ static pfg_status maybe_reset_epochs(pfg_solver* s) {
 // Enqueues one run on the solver's stream. h_srcs (host) or d_srcs (device).
 static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint32_t* d_srcs,
                               uint32_t k, int32_t astar, uint32_t dst, const pfg_options* opt_in,
-                              bool timed) {
+                              bool timed, float* d_trace = nullptr, u32 trace_cap = 0) {
     if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
     pfg_options o = opt_in ? *opt_in : default_options();
     sanitize_options(o);
@@ -530,6 +533,8 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     p.policy = (mode == MODE_DELTA && o.policy == PFG_POLICY_LEARNED) ? 1 : 0;
     p.eager = eager_rounds_for(o);
     p.net = s->d_net;
+    p.trace = mode == MODE_DELTA ? d_trace : nullptr;
+    p.trace_cap = trace_cap;
     p.timeout_ns = device_timeout_ns();
 
     const int map = mode == MODE_NAIVE ? PFG_MAP_THREAD : o.mapping;
@@ -626,6 +631,31 @@ extern "C" pfg_status pfg_run(pfg_solver* s, const uint32_t* h_srcs, uint32_t k,
                                  cudaMemcpyDeviceToHost, s->stream));
         PFG_CUDA(cudaStreamSynchronize(s->stream));
     }
+    return PFG_OK;
+}
+
+extern "C" pfg_status pfg_run_traced(pfg_solver* s, const uint32_t* h_srcs, uint32_t k,
+                                     const pfg_options* opt, pfg_stats* stats_out, float* h_trace,
+                                     uint32_t trace_cap, uint32_t* rows_out, float* ms_out) {
+    if (!s || !h_srcs || !h_trace || !rows_out || trace_cap == 0)
+        return fail(PFG_ERR_INVALID_ARGUMENT, "pfg_run_traced: bad argument");
+    PFG_CUDA(cudaSetDevice(s->device));
+    if (s->pending) complete_run(s, nullptr);
+    if (trace_cap > s->trace_cap) {
+        if (s->d_trace) cudaFree(s->d_trace);
+        s->d_trace = nullptr;
+        s->trace_cap = 0;
+        PFG_CUDA(cudaMalloc((void**)&s->d_trace, (size_t)trace_cap * TRACE_W * sizeof(float)));
+        s->trace_cap = trace_cap;
+    }
+    pfg_status st = enqueue_run(s, h_srcs, nullptr, k, 0, 0, opt, true, s->d_trace, trace_cap);
+    if (st != PFG_OK) return st;
+    st = complete_run(s, stats_out);
+    if (st != PFG_OK) return st;
+    if (ms_out) PFG_CUDA(cudaEventElapsedTime(ms_out, s->ev0, s->ev1));
+    const u32 rows = std::min(s->h_ctl->buckets, trace_cap);
+    *rows_out = rows;
+    if (rows) PFG_CUDA(cudaMemcpy(h_trace, s->d_trace, (size_t)rows * TRACE_W * sizeof(float), cudaMemcpyDeviceToHost));
     return PFG_OK;
 }
 

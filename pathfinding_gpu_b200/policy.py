@@ -1,0 +1,158 @@
+"""Learned Delta policy: trace collection, training and inference (GPU kernels in pfg_policy.cu).
+
+At every decision point of Delta-stepping (the first bucket and every bucket
+advance) the persistent kernel computes 12 features of the frontier and the
+graph (see decision_features in pfg_kernels.cu) and, with the policy loaded,
+evaluates a 12 -> 64 -> 64 -> 64 -> 8 MLP whose argmax picks the next bucket's
+Delta as MULTIPLIERS[c] x the automatic Delta. The policy changes the schedule
+only; distances and parents are identical to the fixed-Delta run.
+
+Training data comes from the solver itself: for each (graph, source) of the
+synthetic families, fixed-Delta runs at every multiplier are timed and traced;
+every trace row of those runs gets the same soft target, a softmax of the
+negative relative run times, so the network learns which Delta class wins from
+what the frontier looks like.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import statistics
+from pathlib import Path
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+from .solver import GpuOptions, GpuSolver, Policy
+
+IN, H, OUT = 12, 64, 8
+TRACE_W = 16
+MULTIPLIERS = [0.25, 0.5, 1.0, 2.0, 4.0, 8.0, 16.0, 64.0]
+SIZES = [("w1", (H, IN)), ("b1", (H,)), ("w2", (H, H)), ("b2", (H,)), ("w3", (H, H)), ("b3", (H,)),
+         ("w4", (OUT, H)), ("b4", (OUT,)), ("in_mean", (IN,)), ("in_scale", (IN,))]
+NP = sum(int(np.prod(s)) for _, s in SIZES)
+WEIGHTS = Path(__file__).resolve().parent / "policy_weights.npz"
+
+
+def init_params(seed: int = 0, mean=None, scale=None) -> np.ndarray:
+    """He-initialised parameter image with the given input normalisation."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for name, shape in SIZES:
+        if name.startswith("w"):
+            parts.append(rng.normal(0, np.sqrt(2.0 / shape[1]), shape))
+        elif name == "in_mean":
+            parts.append(np.zeros(IN) if mean is None else np.asarray(mean))
+        elif name == "in_scale":
+            parts.append(np.ones(IN) if scale is None else np.asarray(scale))
+        else:
+            parts.append(np.zeros(shape))
+    flat = np.concatenate([np.asarray(p, np.float64).reshape(-1) for p in parts]).astype(np.float32)
+    assert flat.size == NP
+    return flat
+
+
+def normalisation(X: np.ndarray):
+    mean = X.mean(axis=0)
+    std = X.std(axis=0)
+    return mean, 1.0 / np.where(std > 1e-6, std, 1.0)
+
+
+def soft_targets(times_ms: Sequence[float], temperature: float = 0.05) -> np.ndarray:
+    t = np.asarray(times_ms, np.float64)
+    r = t / t.min() - 1.0
+    e = np.exp(-r / temperature)
+    return (e / e.sum()).astype(np.float32)
+
+
+def grad(params, X, Y):
+    lib = N.load()
+    params = np.ascontiguousarray(params, np.float32)
+    X = np.ascontiguousarray(X, np.float32)
+    Y = np.ascontiguousarray(Y, np.float32)
+    g = np.empty(NP, np.float32)
+    loss = C.c_float()
+    N.check(lib.pfg_policy_grad(N.ptr(params, N.f32), N.ptr(X, N.f32), N.ptr(Y, N.f32), len(X),
+                                N.ptr(g, N.f32), C.byref(loss)))
+    return float(loss.value), g
+
+
+def train(X, Y, steps: int = 1500, lr: float = 3e-3, seed: int = 0,
+          params: Optional[np.ndarray] = None) -> Tuple[np.ndarray, np.ndarray]:
+    """Full-batch Adam on the GPU; returns (params, per-step loss)."""
+    lib = N.load()
+    X = np.ascontiguousarray(X, np.float32)
+    Y = np.ascontiguousarray(Y, np.float32)
+    if params is None:
+        mean, scale = normalisation(X)
+        params = init_params(seed, mean, scale)
+    params = np.ascontiguousarray(params, np.float32).copy()
+    losses = np.empty(steps, np.float32)
+    N.check(lib.pfg_policy_train(N.ptr(params, N.f32), N.ptr(X, N.f32), N.ptr(Y, N.f32), len(X), steps,
+                                 float(lr), N.ptr(losses, N.f32)))
+    return params, losses
+
+
+def infer(params, X) -> np.ndarray:
+    lib = N.load()
+    params = np.ascontiguousarray(params, np.float32)
+    X = np.ascontiguousarray(X, np.float32)
+    out = np.empty(len(X), np.uint32)
+    N.check(lib.pfg_policy_infer(N.ptr(params, N.f32), N.ptr(X, N.f32), len(X), N.ptr(out, N.u32)))
+    return out
+
+
+def run_traced(solver: GpuSolver, src: int, opt: GpuOptions, cap: int = 4096):
+    """One traced Delta-stepping run: (stats, ms, trace rows [r, 16])."""
+    lib = N.load()
+    from .solver import GpuStats
+    srcs = np.ascontiguousarray([src], np.uint32)
+    c = opt.to_c()
+    st = N.PfgStats()
+    buf = np.empty((cap, TRACE_W), np.float32)
+    rows = C.c_uint32()
+    ms = C.c_float()
+    N.check(lib.pfg_run_traced(solver.handle, N.ptr(srcs, N.u32), 1, C.byref(c), C.byref(st),
+                               N.ptr(buf, N.f32), cap, C.byref(rows), C.byref(ms)))
+    return GpuStats.from_c(st), float(ms.value), buf[: rows.value].copy()
+
+
+def collect(solver: GpuSolver, sources: Iterable[int], reps: int = 3, rows_per_run: int = 96,
+            base: Optional[GpuOptions] = None, seed: int = 0):
+    """Traces and soft targets from fixed-Delta sweeps over MULTIPLIERS."""
+    rng = np.random.default_rng(seed)
+    base = base or GpuOptions()
+    auto = solver.autoDelta()
+    X, Y, table = [], [], []
+    for src in sources:
+        times, traces = [], []
+        for mult in MULTIPLIERS:
+            d = max(1, int(round(auto * mult)))
+            o = GpuOptions(**{**base.__dict__, "delta": d, "policy": Policy.Fixed})
+            solver.run_state([src], o, copy=False)  # warm
+            ts = []
+            tr = None
+            for r in range(reps):
+                st, ms, rows = run_traced(solver, int(src), o)
+                ts.append(ms)
+                tr = rows
+            times.append(statistics.median(ts))
+            if len(tr) > rows_per_run:
+                tr = tr[np.sort(rng.choice(len(tr), rows_per_run, replace=False))]
+            traces.append(tr)
+        y = soft_targets(times)
+        for tr in traces:
+            X.append(tr[:, :IN])
+            Y.append(np.repeat(y[None, :], len(tr), axis=0))
+        table.append({"src": int(src), "times_ms": [round(t, 4) for t in times],
+                      "best": MULTIPLIERS[int(np.argmin(times))]})
+    return np.concatenate(X), np.concatenate(Y), table
+
+
+def save(params: np.ndarray, path: Path = WEIGHTS, meta: Optional[dict] = None) -> None:
+    np.savez(path, params=np.asarray(params, np.float32), meta=np.asarray(str(meta or {})))
+
+
+def load(path: Path = WEIGHTS) -> np.ndarray:
+    d = np.load(path)
+    return d["params"].astype(np.float32)

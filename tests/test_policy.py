@@ -1,0 +1,89 @@
+"""The learned Delta policy on the GPU: gradients of the hand-written training kernels
+against the fp64 oracle, training reduces the loss, inference matches the oracle,
+and a policy-scheduled run is bit-exact and (with the trained weights) faster than
+the fixed automatic Delta."""
+import statistics
+
+import numpy as np
+import pytest
+
+import pathfinding_gpu_b200 as pf
+from pathfinding_gpu_b200 import GpuOptions, Policy
+from pathfinding_gpu_b200 import policy as P
+from oracle import policy_oracle as PO
+
+pytestmark = pytest.mark.gpu
+
+
+def data(n=300, seed=1):
+    rng = np.random.default_rng(seed)
+    X = rng.normal(size=(n, P.IN)).astype(np.float32)
+    Y = rng.dirichlet(np.ones(P.OUT) * 0.5, size=n).astype(np.float32)
+    return X, Y
+
+
+def test_gpu_gradient_matches_oracle():
+    X, Y = data()
+    params = P.init_params(5, X.mean(0), 1 / X.std(0))
+    loss, g = P.grad(params, X, Y)
+    g_ref = PO.grad(params.astype(np.float64), X.astype(np.float64), Y.astype(np.float64))
+    l_ref = PO.loss(params.astype(np.float64), X.astype(np.float64), Y.astype(np.float64))
+    assert abs(loss - l_ref) <= 1e-4 * max(1.0, abs(l_ref))
+    # fp32 accumulation over 300 samples: relative to the largest gradient entry
+    np.testing.assert_allclose(g, g_ref, rtol=0, atol=2e-4 * np.abs(g_ref).max())
+
+
+def test_gpu_training_reduces_loss_and_inference_matches_oracle():
+    X, Y = data(500, 2)
+    # a learnable target: class = argmax of two features
+    Y = np.zeros_like(Y)
+    Y[np.arange(len(X)), (X[:, 0] > 0).astype(int) * 4 + (X[:, 1] > 0).astype(int)] = 1.0
+    params, losses = P.train(X, Y, steps=400, lr=3e-3)
+    assert losses[-1] < 0.5 * losses[0]
+    cls = P.infer(params, X)
+    assert np.array_equal(cls, PO.predict(params.astype(np.float64), X.astype(np.float64)))
+    assert np.mean(cls == np.argmax(Y, 1)) > 0.9
+
+
+def test_traced_run_rows_and_learned_run_is_bit_exact(oracle):
+    g = pf.rmat(12, 16, seed=9)
+    with pf.GpuSolver(g, 1) as s:
+        src = int(pf.pick_sources(g, 1, 3)[0])
+        st, ms, rows = P.run_traced(s, src, GpuOptions(delta=16))
+        assert rows.shape[1] == P.TRACE_W and len(rows) == st.buckets
+        assert np.all(np.isfinite(rows))
+        assert rows[0, 12] == 0 and rows[-1, 12] == len(rows) - 1  # decision index
+        params = P.init_params(7, rows[:, :12].mean(0), 1 / (rows[:, :12].std(0) + 1e-3))
+        s.set_policy(params)
+        r = s.sssp(src, GpuOptions(policy=Policy.Learned))
+        d_ref, p_can = oracle.sssp_canonical(g, src)
+        assert np.array_equal(r.dist, d_ref) and np.array_equal(r.parent, p_can)
+
+
+def test_learned_policy_requires_a_network():
+    g = pf.grid(10, 10, 1)
+    with pf.GpuSolver(g, 1) as s:
+        with pytest.raises(RuntimeError):
+            s.sssp(0, GpuOptions(policy=Policy.Learned))
+
+
+@pytest.mark.skipif(not P.WEIGHTS.exists(), reason="trained weights not present")
+def test_trained_policy_beats_fixed_delta_on_rmat20(oracle):
+    params = P.load()
+    g = pf.rmat(20, 16, seed=2026)
+    with pf.GpuSolver(g, 1) as s:
+        s.set_policy(params)
+        src = int(pf.pick_sources(g, 1, 2026)[0])
+        fixed = GpuOptions(blockSize=1024)
+        learned = GpuOptions(blockSize=1024, policy=Policy.Learned)
+        for o in (fixed, learned):
+            s.run_state([src], o, copy=False)
+        tf = statistics.median(s.run_state([src], fixed, copy=False)[1] for _ in range(5))
+        tl = statistics.median(s.run_state([src], learned, copy=False)[1] for _ in range(5))
+        _, _, a = s.run_state([src], fixed)
+        _, _, b = s.run_state([src], learned)
+        assert np.array_equal(a, b)
+        d_ref, p_can = oracle.sssp_canonical(g, src)
+        d, p = pf.unpack(b)
+        assert np.array_equal(d, d_ref) and np.array_equal(p, p_can)
+        assert tf / tl >= 1.3, (tf, tl)
