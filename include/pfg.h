@@ -224,6 +224,39 @@ PFG_API void* pfg_batch_stream(const pfg_batch* b);
 PFG_API double pfg_batch_upload_ms(const pfg_batch* b);
 PFG_API uint64_t pfg_batch_device_bytes(const pfg_batch* b);
 
+/* ---- serving: continuous batching of A* queries (extension; the reference
+ *      answers one query per GpuSolver::astar call, src/gpu_sssp.cu:549-551) ----
+ * The graph and `slots` query slots stay resident. pfg_server_submit queues a
+ * query on the host; every pfg_server_step admits queued queries into free
+ * slots, runs at most max_rounds device rounds of one persistent launch that
+ * relaxes every slot in flight together (queries admitted later join the
+ * shared bucket sequence at its next bucket), and retires the slots whose
+ * search is complete. Finished queries are drained with pfg_server_results;
+ * times are microseconds since the server was created. dist is the exact
+ * shortest distance (PFG_INF if unreachable). */
+typedef struct pfg_server pfg_server;
+typedef struct pfg_query_result {
+    uint64_t id;
+    uint32_t src, dst, dist, slot;
+    double submit_us, admit_us, finish_us;
+} pfg_query_result;
+PFG_API pfg_status pfg_server_create(const uint32_t* row_offsets, const uint32_t* col_indices,
+                                     const uint32_t* weights, const double* x, const double* y,
+                                     uint32_t n, uint32_t m, double h_scale, double avg_w,
+                                     double avg_deg, uint32_t slots, const pfg_options* opt,
+                                     int32_t device, pfg_server** out);
+PFG_API void pfg_server_destroy(pfg_server* v);
+PFG_API pfg_status pfg_server_submit(pfg_server* v, uint32_t src, uint32_t dst, uint64_t* id_out);
+PFG_API pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32_t* admitted_out,
+                                   uint32_t* completed_out);
+PFG_API pfg_status pfg_server_results(pfg_server* v, pfg_query_result* out, uint32_t cap,
+                                      uint32_t* n_out);
+PFG_API uint32_t pfg_server_pending(const pfg_server* v);
+PFG_API uint32_t pfg_server_in_flight(const pfg_server* v);
+PFG_API double pfg_server_now_us(const pfg_server* v);
+/* The server's solver (graph + slots), e.g. to load a policy network. */
+PFG_API pfg_solver* pfg_server_solver(pfg_server* v);
+
 /* ---- learned Delta policy (extension; no reference counterpart) ----
  * The policy is a 12 -> 64 -> 64 -> 64 -> 8 fp32 MLP evaluated on the device
  * at every bucket advance; its argmax picks the next bucket's Delta as one of

@@ -52,8 +52,23 @@ class PfgGraphInfo(C.Structure):
                 ("has_xy", i32), ("avg_w", f64), ("avg_deg", f64), ("h_scale", f64)]
 
 
+class PfgQueryResult(C.Structure):
+    _fields_ = [("id", u64), ("src", u32), ("dst", u32), ("dist", u32), ("slot", u32),
+                ("submit_us", f64), ("admit_us", f64), ("finish_us", f64)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/*.h
 SIGNATURES = {
+    "pfg_server_create": (i32, [P(u32), P(u32), P(u32), P(f64), P(f64), u32, u32, f64, f64, f64, u32,
+                                P(PfgOptions), i32, P(C.c_void_p)]),
+    "pfg_server_destroy": (None, [C.c_void_p]),
+    "pfg_server_submit": (i32, [C.c_void_p, u32, u32, P(u64)]),
+    "pfg_server_step": (i32, [C.c_void_p, u32, P(u32), P(u32)]),
+    "pfg_server_results": (i32, [C.c_void_p, P(PfgQueryResult), u32, P(u32)]),
+    "pfg_server_pending": (u32, [C.c_void_p]),
+    "pfg_server_in_flight": (u32, [C.c_void_p]),
+    "pfg_server_now_us": (f64, [C.c_void_p]),
+    "pfg_server_solver": (C.c_void_p, [C.c_void_p]),
     # include/pfg.h
     "pfg_create": (i32, [P(u32), P(u32), P(u32), P(f64), P(f64), u32, u32, f64, f64, f64, u32,
                          P(C.c_void_p)]),

@@ -23,8 +23,8 @@ NVCC_FLAGS = ARCH + [
     "-I", str(ROOT / "include"),
 ]
 SOURCES = ["pfg_kernels.cu", "pfg_solver.cu", "pfg_device.cu", "pfg_policy.cu", "pfg_batch.cu",
-           "pfg_noalloc.cu", "pfg_graphs.cpp"]
-HEADERS = ["pfg_common.cuh", "pfg_kernels.h"]
+           "pfg_serve.cu", "pfg_noalloc.cu", "pfg_graphs.cpp"]
+HEADERS = ["pfg_common.cuh", "pfg_kernels.h", "pfg_internal.h"]
 
 
 def _nvcc() -> str:

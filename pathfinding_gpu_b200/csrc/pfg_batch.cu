@@ -315,6 +315,7 @@ static pfg_status batch_prepare(pfg_batch* b, const pfg_options* opt_in, RunPara
     p.mode = mode;
     p.prefix_scan = (mode == MODE_FRONTIER && o.compaction == PFG_COMPACT_PREFIX_SCAN) ? 1 : 0;
     p.eager = eager_rounds_for(o);
+    if (o.eager < 0 && b->avg_deg > 6.0) p.eager = 0;  // as the single-graph solver: road-like graphs only
     p.timeout_ns = device_timeout_ns();
     block = o.block_size;
     const int bps = blocks_per_sm_for(o, false, o.mapping);

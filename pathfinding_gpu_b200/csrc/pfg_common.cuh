@@ -40,7 +40,8 @@ enum Phase : u32 {
     PH_HEAVY = 3,  // relax heavy arcs of the bucket's settled set R
     PH_NAIVE = 4,  // Bellman-Ford sweep over all vertices (naive mode)
     PH_COMPACT = 5,// prefix-sum compaction of the flagged next frontier
-    PH_DONE = 6
+    PH_DONE = 6,
+    PH_PAUSE = 7   // serving: the step's round budget is spent; Ctl::resume_phase is next
 };
 
 // Run modes (reference GpuAlgo, include/gpu_sssp.h:10-14).
@@ -81,7 +82,9 @@ struct __align__(16) Ctl {
     u32 policy_calls;  // learned-policy decisions taken
     u32 bucket_near;   // items entering the current bucket (policy feature)
     u32 bucket_rounds; // rounds spent in the current bucket (policy feature)
-    u32 pad_c0, pad_c1, pad_c2;
+    u32 step_left;     // serving: rounds left in this step
+    u32 resume_phase;  // serving: phase to run when a paused machine resumes
+    u32 pad_c2;
     u64 far_min[2];    // smallest key pushed to each far pile
     u32 cnt[C_COUNT];  // queue tails
     unsigned long long stats[4];  // edges, atomics, updates, pushes
@@ -147,6 +150,21 @@ struct RunParams {
     // prow[inst_rowbase[i]]. nullptr: uniform instances of one graph, i*n + v.
     const u32* inst_off;
     const u32* inst_rowbase;
+    // Serving (continuous batching of A* queries on uniform slots i*n + v):
+    // slot i searches from its source to inst_target[i]; its keys are
+    // dist + h_i(v) + inst_phi[i], so a query admitted later enters the shared
+    // bucket sequence at the current window. inst_far_cnt[i] counts the slot's
+    // items in the far pile of the current bucket; a slot with none left at a
+    // bucket advance is finished (inst_done[i] = round + 1).
+    const u32* inst_target;
+    const double* inst_tx;
+    const double* inst_ty;
+    const long long* inst_phi;
+    u32* inst_far_cnt;
+    u32* inst_active;
+    u32* inst_done;
+    u32 step_rounds;   // > 0: pause after this many rounds (serving steps)
+    int resume;        // 1: continue a paused state machine instead of starting a run
     u32 eager;         // hybrid mapping: eager sub-rounds per round (0 = off)
     u32 eager_max_items;  // ... only in rounds whose input has at most this many items
     const PolicyNet* net;

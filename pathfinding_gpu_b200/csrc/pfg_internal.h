@@ -6,6 +6,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 namespace pfg {
 
 // Records the calling thread's error message and returns `st`.
@@ -35,3 +37,70 @@ u32 eager_rounds_for(const pfg_options& o);
 u64 device_timeout_ns();
 
 }  // namespace pfg
+
+#include <string>
+#include <vector>
+
+// One solver: the graph and the working set of max_batch instances on one device.
+struct pfg_solver {
+    typedef pfg::u32 u32;
+    typedef pfg::u64 u64;
+    typedef pfg::Ctl Ctl;
+    typedef pfg::PolicyNet PolicyNet;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    u32 n = 0, m = 0, K = 1, maxw = 0;
+    u64 m_pad = 0;
+    double hscale = 0.0, avg_w = 0.0, avg_deg = 0.0;
+    bool has_xy = false;
+    std::vector<double> hx, hy;  // host copies of the coordinates (A* target lookup)
+    int sm_count = 1;
+    double upload_ms = 0.0;
+    u64 bytes = 0;
+
+    uint2* d_adj = nullptr;
+    u32* d_prow = nullptr;
+    double* d_x = nullptr;
+    double* d_y = nullptr;
+    u64* d_state = nullptr;
+    u32* d_q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // near0, near1, far0, far1, R
+    u32* d_stamp[3] = {nullptr, nullptr, nullptr};                // near, far, R
+    u32* d_naive[2] = {nullptr, nullptr};
+    u32* d_srcs = nullptr;
+    u32* d_path = nullptr;      // path extraction scratch [n + 1]
+    u32* d_path_len = nullptr;
+    Ctl* d_ctl = nullptr;
+    PolicyNet* d_net = nullptr;
+    bool has_net = false;
+    float* d_trace = nullptr;   // per-bucket policy features of traced runs
+    u32 trace_cap = 0;
+
+    Ctl* h_ctl = nullptr;       // pinned mirror of the control block
+    u32* h_srcs = nullptr;      // pinned staging of the sources [K]
+
+    // last asynchronous run
+    bool pending = false;
+    pfg_status pending_status = PFG_OK;
+    int last_mode = pfg::MODE_DELTA;
+    u32 last_delta = 0;
+    u32 last_k = 0;
+    u32 epoch_hint = 1;   // largest epoch known to the host (stamps reset near 2^32)
+    std::vector<void*> allocs;
+
+    template <class T>
+    pfg_status dalloc(T** p, u64 count) {
+        void* q = nullptr;
+        const u64 b = std::max<u64>(1, count) * sizeof(T);
+        cudaError_t e = cudaMalloc(&q, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return pfg::set_error(PFG_ERR_OUT_OF_MEMORY, "cudaMalloc of %.1f MB failed: %s", b / 1048576.0,
+                        cudaGetErrorString(e));
+        }
+        allocs.push_back(q);
+        bytes += b;
+        *p = (T*)q;
+        return PFG_OK;
+    }
+};

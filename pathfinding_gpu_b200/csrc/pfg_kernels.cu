@@ -54,7 +54,8 @@ struct Coop {
     u32 u[MAX_BS];
     u32 du[MAX_BS];
     u32 ib[MAX_BS];
-    u32 ub[MAX_BS];
+    u32 inst[MAX_BS];
+    u64 ub[MAX_BS];
     u32 wsum[32];
     u32 cl[CL_CAP];  // near vertices claimed by this CTA in the current round
     u32 cl_n;        // entries appended (may exceed CL_CAP; the excess went to the global queue)
@@ -116,6 +117,26 @@ __device__ __forceinline__ u32 h_of(const RunParams& p, u32 v) {
     return heuristic_value(p.x[v], p.y[v], p.xt, p.yt, p.hscale);
 }
 
+// A* key of a vertex of instance `inst` at distance d: d + h(v) + phi, where the
+// target (and so h) and the key offset phi are per instance when serving.
+__device__ __forceinline__ u64 astar_key(const RunParams& p, u32 inst, u32 v, u64 d) {
+    if (!p.use_h) return p.inst_phi ? (u64)((long long)d + __ldg(p.inst_phi + inst)) : d;
+    if (p.inst_target) {
+        const u32 h = heuristic_value(p.x[v], p.y[v], __ldg(p.inst_tx + inst), __ldg(p.inst_ty + inst), p.hscale);
+        return (u64)((long long)d + (long long)h + __ldg(p.inst_phi + inst));
+    }
+    return d + heuristic_value(p.x[v], p.y[v], p.xt, p.yt, p.hscale);
+}
+
+// Pruning bound of an A* instance in key space: key(target) = dist(target) + phi
+// (h(target) = 0), or "none" while the target is unreached.
+__device__ __forceinline__ u64 astar_bound(const RunParams& p, u32 inst, u32 ib) {
+    const u32 t = p.inst_target ? __ldg(p.inst_target + inst) : p.target;
+    const u32 dt = st_dist(ld_state(p.state + ib + t));
+    if (dt == INF32) return ~0ull;
+    return p.inst_phi ? (u64)((long long)dt + __ldg(p.inst_phi + inst)) : (u64)dt;
+}
+
 // First arc of [r0, r1) whose weight exceeds delta (rows are sorted by weight).
 __device__ __forceinline__ u32 light_end(const uint2* adj, u32 r0, u32 r1, u32 delta) {
     u32 lo = r0, hi = r1;
@@ -135,14 +156,14 @@ __device__ __forceinline__ u32 light_end(const uint2* adj, u32 r0, u32 r1, u32 d
 // round; only overflow goes to the global queue directly.
 template <bool ASTAR, int AM>
 __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32 u, u32 du,
-                                          u32 ib, u32 ub, u32 v, u32 w, Local& L, Coop* cl) {
+                                          u32 ib, u64 ub, u32 inst, u32 v, u32 w, Local& L, Coop* cl) {
     if (w == PAD_W) return;
     L.edges++;
     const u64 nd = (u64)du + w;
     if (nd >= INF32) return;
     u64 key = nd;
     if constexpr (ASTAR) {
-        key += h_of(p, v);
+        key = astar_key(p, inst, v, nd);
         if (key >= ub) return;  // f(v) >= dist[target]: cannot improve the answer
     }
     const u32 gv = ib + v;
@@ -171,6 +192,7 @@ __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32
         if (claim_stamp(p.far_stamp, gv, s.far_epoch)) {
             queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gv);
             L.pushes++;
+            if (p.inst_far_cnt) atomicAdd(p.inst_far_cnt + inst, 1u);
         }
         L.fmin = key < L.fmin ? key : L.fmin;
     }
@@ -180,12 +202,12 @@ __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32
 // (two arcs per load; rows start on 32-byte boundaries).
 template <bool ASTAR, int AM>
 __device__ __forceinline__ void relax_range_thread(const RunParams& p, const Snap& s, u32 u, u32 du,
-                                                   u32 ib, u32 ub, u32 eb, u32 ee, Local& L) {
+                                                   u32 ib, u64 ub, u32 inst, u32 eb, u32 ee, Local& L) {
     const uint4* a4 = reinterpret_cast<const uint4*>(p.adj);
     for (u32 e = eb & ~1u; e < ee; e += 2) {
         const uint4 q = __ldg(a4 + (e >> 1));
-        if (e >= eb) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, q.x, q.y, L, nullptr);
-        if (e + 1 < ee) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, q.z, q.w, L, nullptr);
+        if (e >= eb) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, inst, q.x, q.y, L, nullptr);
+        if (e + 1 < ee) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, inst, q.z, q.w, L, nullptr);
     }
 }
 
@@ -195,8 +217,8 @@ __device__ __forceinline__ void relax_range_thread(const RunParams& p, const Sna
 // [eb, ee) is the arc range of the round kind (light prefix / heavy suffix).
 template <bool ASTAR>
 __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32 gi, int kind,
-                                          Local& L, u32& u, u32& ib, u32& du, u32& ub, u32& eb,
-                                          u32& ee) {
+                                          Local& L, u32& u, u32& ib, u32& du, u64& ub, u32& inst,
+                                          u32& eb, u32& ee) {
     Ctl* c = p.ctl;
     u32 rb = 0;  // first padded row start of the item's graph
     if (p.inst_off) {
@@ -206,10 +228,11 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
             const u32 mid = (lo + hi + 1) >> 1;
             if (__ldg(p.inst_off + mid) <= gi) lo = mid; else hi = mid - 1;
         }
+        inst = lo;
         ib = __ldg(p.inst_off + lo);
         rb = __ldg(p.inst_rowbase + lo);
     } else {
-        const u32 inst = p.k > 1 ? gi / p.n : 0u;
+        inst = p.k > 1 ? gi / p.n : 0u;
         ib = inst * p.n;
     }
     u = gi - ib;
@@ -217,9 +240,9 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
     bool act = du != INF32;
     u64 key = du;
     if constexpr (ASTAR) {
-        ub = st_dist(ld_state(p.state + ib + p.target));
+        ub = astar_bound(p, inst, ib);
         if (act) {
-            key += h_of(p, u);
+            key = astar_key(p, inst, u, du);
             if (key >= ub) act = false;
         }
     }
@@ -231,6 +254,7 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
             if (claim_stamp(p.far_stamp, gi, s.far_epoch)) {
                 queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gi);
                 L.pushes++;
+                if (p.inst_far_cnt) atomicAdd(p.inst_far_cnt + inst, 1u);
             }
             L.fmin = key < L.fmin ? key : L.fmin;
         }
@@ -260,8 +284,8 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
 // (one dependent chain per arc). Called by every thread of the CTA.
 template <bool ASTAR, int AM>
 __device__ __forceinline__ void relax_chunk_edges(const RunParams& p, const Snap& s, bool act, u32 u,
-                                                  u32 du, u32 ib, u32 ub, u32 eb, u32 ee, Local& L,
-                                                  Coop& cs, Coop* cl) {
+                                                  u32 du, u32 ib, u64 ub, u32 inst, u32 eb, u32 ee,
+                                                  Local& L, Coop& cs, Coop* cl) {
     const u32 BS = blockDim.x;
     u32 total = 0;
     const u32 sz = act ? ee - eb : 0u;
@@ -273,6 +297,7 @@ __device__ __forceinline__ void relax_chunk_edges(const RunParams& p, const Snap
     cs.du[threadIdx.x] = du;
     cs.ib[threadIdx.x] = ib;
     cs.ub[threadIdx.x] = ub;
+    cs.inst[threadIdx.x] = inst;
     if (threadIdx.x == 0) cs.off[BS] = total;
     __syncthreads();
     for (u32 j = threadIdx.x; j < total; j += BS) {
@@ -286,7 +311,7 @@ __device__ __forceinline__ void relax_chunk_edges(const RunParams& p, const Snap
         }
         const u32 e = cs.eb[lo] + (j - cs.off[lo]);
         const uint2 a = __ldg(p.adj + e);
-        relax_arc<ASTAR, AM>(p, s, cs.u[lo], cs.du[lo], cs.ib[lo], cs.ub[lo], a.x, a.y, L, cl);
+        relax_arc<ASTAR, AM>(p, s, cs.u[lo], cs.du[lo], cs.ib[lo], cs.ub[lo], cs.inst[lo], a.x, a.y, L, cl);
     }
     __syncthreads();
 }
@@ -322,12 +347,14 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
     const u32 send = min(count, sbeg + per);
     for (u32 base = sbeg; base < send; base += BS) {
         const u32 idx = base + threadIdx.x;
-        u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, ub = INF32;
+        u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, inst = 0;
+        u64 ub = ~0ull;
         bool act = false;
-        if (idx < send) act = take_item<ASTAR>(p, s, ld_cg(in + idx), kind, L, u, ib, du, ub, eb, ee);
+        if (idx < send)
+            act = take_item<ASTAR>(p, s, ld_cg(in + idx), kind, L, u, ib, du, ub, inst, eb, ee);
 
         if constexpr (MAP == 0) {  // thread per item
-            if (act) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, eb, ee, L);
+            if (act) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, inst, eb, ee, L);
         } else if constexpr (MAP == 1) {  // warp per item
             const u32 lane = threadIdx.x & 31u;
             unsigned ballot = __ballot_sync(FULL, act);
@@ -335,15 +362,16 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
                 const int leader = __ffs(ballot) - 1;
                 ballot &= ballot - 1;
                 const u32 wu = __shfl_sync(FULL, u, leader), wdu = __shfl_sync(FULL, du, leader);
-                const u32 wib = __shfl_sync(FULL, ib, leader), wub = __shfl_sync(FULL, ub, leader);
+                const u32 wib = __shfl_sync(FULL, ib, leader), winst = __shfl_sync(FULL, inst, leader);
+                const u64 wub = __shfl_sync(FULL, ub, leader);
                 const u32 web = __shfl_sync(FULL, eb, leader), wee = __shfl_sync(FULL, ee, leader);
                 for (u32 e = web + lane; e < wee; e += 32) {
                     const uint2 a = __ldg(p.adj + e);
-                    relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, a.x, a.y, L, nullptr);
+                    relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, winst, a.x, a.y, L, nullptr);
                 }
             }
         } else {
-            relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, eb, ee, L, cs, cl);
+            relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
         }
     }
     if constexpr (MAP == 2) {
@@ -365,11 +393,12 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
                     if (hi <= lo) break;  // block-uniform
                     for (u32 base = lo; base < hi; base += BS) {
                         const u32 idx = base + threadIdx.x;
-                        u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, ub = INF32;
+                        u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, inst = 0;
+                        u64 ub = ~0ull;
                         bool act = false;
                         if (idx < hi)
-                            act = take_item<ASTAR>(p, s, cs.cl[idx], K_LIGHT, L, u, ib, du, ub, eb, ee);
-                        relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, eb, ee, L, cs, cl);
+                            act = take_item<ASTAR>(p, s, cs.cl[idx], K_LIGHT, L, u, ib, du, ub, inst, eb, ee);
+                        relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
                     }
                     lo = hi;
                 }
@@ -670,9 +699,27 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
                 s_flag[0] = p.policy ? 1u : 2u;
                 if (p.policy || p.trace) decision_features(p, sc, r, fn, est, s_feat);
             }
+            s_flag[2] = p.inst_far_cnt ? 1u : 0u;
+        } else {
+            s_flag[2] = 0u;
         }
     }
     __syncthreads();
+    if (s_flag[2]) {
+        // Serving: at a bucket advance the near queue is empty, so a slot with
+        // no item in the far pile has nothing left to relax - its target
+        // distance is final (or the target is unreachable). Counts restart for
+        // the next bucket (its SCAN round recounts the items it keeps).
+        const bool all_done = sc.rd.phase == PH_DONE;
+        for (u32 i = t; i < p.k; i += blockDim.x) {
+            if (p.inst_active[i] && (all_done || p.inst_far_cnt[i] == 0u)) {
+                p.inst_active[i] = 0u;
+                p.inst_done[i] = sc.rounds;
+            }
+            p.inst_far_cnt[i] = 0u;
+        }
+        __threadfence();
+    }
     const u32 need = s_flag[0];
     if (need == 1u || need == 3u) {
         const u32 cls = policy_pick(p.net, s_feat, act0, act1);
@@ -720,6 +767,16 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
         sc.near_epoch = r.near_epoch;
         sc.far_epoch = r.far_epoch;
         sc.r_epoch = r.r_epoch;
+        // serving steps: pause when the step's round budget is spent
+        if (p.step_rounds && r.phase != PH_DONE) {
+            if (sc.step_left <= 1u) {
+                sc.resume_phase = r.phase;
+                r.phase = PH_PAUSE;
+                sc.step_left = 0u;
+            } else {
+                sc.step_left -= 1u;
+            }
+        }
     }
     __syncthreads();
 }
@@ -811,23 +868,36 @@ __global__ void __launch_bounds__(MAX_BS) k_persistent(const __grid_constant__ R
     __shared__ Coop cs;
     __shared__ Ctl sc;
     __shared__ u64 red[32];
-    __shared__ u32 s_flag[2];
+    __shared__ u32 s_flag[3];
     __shared__ float s_feat[POL_IN];
     __shared__ float act0[POL_H], act1[POL_H];
     Local L;
 
-    // INIT: every state word to (INF, NO_PARENT) (reference initStateKernel,
-    // src/gpu_kernels.cuh:334-337).
-    const u64 gtid = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    const u64 gstride = (u64)gridDim.x * blockDim.x;
-    for (u64 i = gtid; i < p.total; i += gstride) p.state[i] = STATE_INIT;
-    if (threadIdx.x == 0) {
-        s.far_out = 0;
-        cs.cl_n = 0;
+    if (p.resume) {
+        // Continue a paused machine (serving): the round descriptor in the
+        // control block is already set for the next round.
+        if (threadIdx.x == 0) {
+            const uint4* src = reinterpret_cast<const uint4*>(&p.ctl->rd);
+            uint4* dst = reinterpret_cast<uint4*>(&s);
+            for (int i = 0; i < 5; ++i) dst[i] = __ldcg(src + i);
+            cs.cl_n = 0;
+            if (s.status != DS_OK) s.phase = PH_DONE;
+        }
+        __syncthreads();
+    } else {
+        // INIT: every state word to (INF, NO_PARENT) (reference initStateKernel,
+        // src/gpu_kernels.cuh:334-337).
+        const u64 gtid = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+        const u64 gstride = (u64)gridDim.x * blockDim.x;
+        for (u64 i = gtid; i < p.total; i += gstride) p.state[i] = STATE_INIT;
+        if (threadIdx.x == 0) {
+            s.far_out = 0;
+            cs.cl_n = 0;
+        }
+        grid_barrier(p, s, L, red, sc, s_flag, s_feat, act0, act1);
     }
-    grid_barrier(p, s, L, red, sc, s_flag, s_feat, act0, act1);
 
-    while (s.phase != PH_DONE) {
+    while (s.phase != PH_DONE && s.phase != PH_PAUSE) {
         const u32 ph = s.phase;
         if (ph == PH_LIGHT) {
             round_items<ASTAR, AM, MAP>(p, s, p.nearq[s.in_buf], s.in_count, K_LIGHT, L, cs);

@@ -79,64 +79,7 @@ extern "C" const char* pfg_status_string(pfg_status st) {
 // ---------------------------------------------------------------------------
 // Solver object
 // ---------------------------------------------------------------------------
-struct pfg_solver {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    u32 n = 0, m = 0, K = 1, maxw = 0;
-    u64 m_pad = 0;
-    double hscale = 0.0, avg_w = 0.0, avg_deg = 0.0;
-    bool has_xy = false;
-    std::vector<double> hx, hy;  // host copies of the coordinates (A* target lookup)
-    int sm_count = 1;
-    double upload_ms = 0.0;
-    u64 bytes = 0;
-
-    uint2* d_adj = nullptr;
-    u32* d_prow = nullptr;
-    double* d_x = nullptr;
-    double* d_y = nullptr;
-    u64* d_state = nullptr;
-    u32* d_q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // near0, near1, far0, far1, R
-    u32* d_stamp[3] = {nullptr, nullptr, nullptr};                // near, far, R
-    u32* d_naive[2] = {nullptr, nullptr};
-    u32* d_srcs = nullptr;
-    u32* d_path = nullptr;      // path extraction scratch [n + 1]
-    u32* d_path_len = nullptr;
-    Ctl* d_ctl = nullptr;
-    PolicyNet* d_net = nullptr;
-    bool has_net = false;
-    float* d_trace = nullptr;   // per-bucket policy features of traced runs
-    u32 trace_cap = 0;
-
-    Ctl* h_ctl = nullptr;       // pinned mirror of the control block
-    u32* h_srcs = nullptr;      // pinned staging of the sources [K]
-
-    // last asynchronous run
-    bool pending = false;
-    pfg_status pending_status = PFG_OK;
-    int last_mode = MODE_DELTA;
-    u32 last_delta = 0;
-    u32 last_k = 0;
-    u32 epoch_hint = 1;   // largest epoch known to the host (stamps reset near 2^32)
-    std::vector<void*> allocs;
-
-    template <class T>
-    pfg_status dalloc(T** p, u64 count) {
-        void* q = nullptr;
-        const u64 b = std::max<u64>(1, count) * sizeof(T);
-        cudaError_t e = cudaMalloc(&q, b);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return fail(PFG_ERR_OUT_OF_MEMORY, "cudaMalloc of %.1f MB failed: %s", b / 1048576.0,
-                        cudaGetErrorString(e));
-        }
-        allocs.push_back(q);
-        bytes += b;
-        *p = (T*)q;
-        return PFG_OK;
-    }
-};
+// struct pfg_solver is defined in pfg_internal.h (shared with the serving engine).
 
 u32 pfg::auto_delta_of(double avg_w, double avg_deg) {
     // Davidson et al.: Delta ~ warp size * average weight / average degree
@@ -391,6 +334,7 @@ static int env_int(const char* name, int dflt) {
 // Eager sub-rounds per grid round of the hybrid mapping when the caller leaves
 // the choice to the engine (pfg_options::eager < 0).
 static const int kDefaultEager = 4;
+static const double kEagerMaxAvgDegree = 6.0;
 
 namespace pfg {
 
@@ -532,6 +476,9 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     p.prefix_scan = (mode == MODE_FRONTIER && o.compaction == PFG_COMPACT_PREFIX_SCAN) ? 1 : 0;
     p.policy = (mode == MODE_DELTA && o.policy == PFG_POLICY_LEARNED) ? 1 : 0;
     p.eager = eager_rounds_for(o);
+    // Engine default: eager propagation only on low-degree (road-like) graphs;
+    // on power-law graphs one hub expands into a burst of redundant work.
+    if (o.eager < 0 && s->avg_deg > kEagerMaxAvgDegree) p.eager = 0;
     p.net = s->d_net;
     p.trace = mode == MODE_DELTA ? d_trace : nullptr;
     p.trace_cap = trace_cap;
