@@ -61,6 +61,14 @@ enum pfg_atomic { PFG_ATOMIC_MIN_RBA = 0, PFG_ATOMIC_CAS_RBA = 1, PFG_ATOMIC_MIN
 enum pfg_compaction { PFG_COMPACT_WARP_ATOMIC = 0, PFG_COMPACT_PREFIX_SCAN = 1 };
 /* Schedule policy for Delta-stepping (extension; no reference counterpart). */
 enum pfg_policy_kind { PFG_POLICY_FIXED = 0, PFG_POLICY_LEARNED = 1 };
+/* How a Delta-stepping bucket is worked off (extension; no reference counterpart).
+ * ROUNDS: relaxation rounds separated by grid barriers (the reference's loop).
+ * ASYNC:  one drain per bucket: CTAs relax the vertices they claim from their
+ *         own shared-memory list and share work through a ring queue, with a
+ *         grid barrier only between buckets.
+ * AUTO:   ASYNC for fixed-Delta Delta-stepping, ROUNDS otherwise (Naive,
+ *         Frontier, learned policy, traced runs, serving steps). */
+enum pfg_schedule { PFG_SCHEDULE_AUTO = 0, PFG_SCHEDULE_ROUNDS = 1, PFG_SCHEDULE_ASYNC = 2 };
 
 /* Mirrors GpuOptions (reference: include/gpu_sssp.h:42-52) plus `policy`. */
 typedef struct pfg_options {
@@ -77,6 +85,8 @@ typedef struct pfg_options {
                             grid round; -1 = engine default, 0 = off (extension) */
     int32_t blocks_per_sm; /* CTAs of the persistent kernel per SM; 0 = engine
                               default (1024 resident threads per SM) (extension) */
+    int32_t schedule;    /* enum pfg_schedule, default PFG_SCHEDULE_AUTO; ASYNC
+                            applies to fixed-Delta runs only (extension)        */
 } pfg_options;
 
 /* Mirrors GpuStats (reference: include/gpu_sssp.h:55-65) plus `rounds`. */

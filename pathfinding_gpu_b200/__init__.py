@@ -4,13 +4,13 @@ from .graphs import (CSRGraph, buildCSR, grid, rmat, road, grid_batch, grid_batc
                      load_dimacs, load_snap, load_binary, pick_sources, uniform_vertices, SplitMix64,
                      DEFAULT_SEED)
 from .solver import (GpuSolver, GpuOptions, GpuStats, GpuRunResult, GpuAlgo, Mapping, AtomicMode,
-                     Compaction, Policy, INF_DIST, NO_PARENT, unpack, reconstruct_path, device_info)
+                     Compaction, Policy, Schedule, INF_DIST, NO_PARENT, unpack, reconstruct_path, device_info)
 from ._native import PfgError
 
 __all__ = [
     "CSRGraph", "buildCSR", "grid", "rmat", "road", "grid_batch", "grid_batch_sides", "union",
     "load_dimacs", "load_snap", "load_binary", "pick_sources", "uniform_vertices", "SplitMix64",
     "DEFAULT_SEED", "GpuSolver", "GpuOptions", "GpuStats", "GpuRunResult", "GpuAlgo", "Mapping",
-    "AtomicMode", "Compaction", "Policy", "INF_DIST", "NO_PARENT", "unpack", "reconstruct_path",
+    "AtomicMode", "Compaction", "Policy", "Schedule", "INF_DIST", "NO_PARENT", "unpack", "reconstruct_path",
     "device_info", "PfgError",
 ]

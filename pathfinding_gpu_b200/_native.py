@@ -26,7 +26,7 @@ STATUS_NAMES = {
 class PfgOptions(C.Structure):
     _fields_ = [("algo", i32), ("mapping", i32), ("atomic", i32), ("delta", u32),
                 ("block_size", i32), ("sync_every", u32), ("compaction", i32), ("policy", i32),
-                ("eager", i32), ("blocks_per_sm", i32)]
+                ("eager", i32), ("blocks_per_sm", i32), ("schedule", i32)]
 
 
 class PfgStats(C.Structure):

@@ -31,6 +31,7 @@ pfg_options to_c(const GpuOptions& o) {
     c.policy = PFG_POLICY_FIXED;
     c.eager = -1;
     c.blocks_per_sm = 0;
+    c.schedule = PFG_SCHEDULE_AUTO;
     return c;
 }
 

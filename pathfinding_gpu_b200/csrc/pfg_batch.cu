@@ -46,6 +46,9 @@ struct pfg_batch {
     u32* d_inst_off = nullptr;
     u32* d_inst_rowbase = nullptr;
     u32* d_srcs = nullptr;
+    u32* d_ring = nullptr;  // ring queue of asynchronous buckets, RING_EMPTY when idle
+    u32 ring_mask = 0;
+    u32* d_aq = nullptr;    // ring counters
     Ctl* d_ctl = nullptr;
     Ctl* h_ctl_init = nullptr;  // pinned: the control block every run starts from
     Ctl* h_ctl_out = nullptr;   // pinned: the control block every run ends with
@@ -190,7 +193,14 @@ static pfg_status batch_create(pfg_batch* b, uint32_t num_graphs, const uint32_t
     if (st == PFG_OK) st = b->dalloc(&b->d_inst_rowbase, b->max_inst);
     if (st == PFG_OK) st = b->dalloc(&b->d_srcs, b->max_inst);
     if (st == PFG_OK) st = b->dalloc(&b->d_ctl, 1);
+    u64 ring = 1024;
+    while (ring < S) ring <<= 1;
+    if (st == PFG_OK) st = b->dalloc(&b->d_ring, ring);
+    if (st == PFG_OK) st = b->dalloc(&b->d_aq, (u64)AQ_WORDS);
     if (st != PFG_OK) return st;
+    b->ring_mask = (u32)(ring - 1);
+    B_CUDA(cudaMemsetAsync(b->d_ring, 0xFF, ring * 4, b->stream));
+    B_CUDA(cudaMemsetAsync(b->d_aq, 0, AQ_WORDS * 4, b->stream));
     for (int i = 0; i < 3; ++i) B_CUDA(cudaMemsetAsync(b->d_stamp[i], 0, S * 4, b->stream));
     B_CUDA(cudaMallocHost((void**)&b->h_ctl_init, sizeof(Ctl)));
     B_CUDA(cudaMallocHost((void**)&b->h_ctl_out, sizeof(Ctl)));
@@ -317,6 +327,11 @@ static pfg_status batch_prepare(pfg_batch* b, const pfg_options* opt_in, RunPara
     p.eager = eager_rounds_for(o);
     if (o.eager < 0 && b->avg_deg > 6.0) p.eager = 0;  // as the single-graph solver: road-like graphs only
     p.timeout_ns = device_timeout_ns();
+    if (async_buckets_for(o, mode, false, false)) {
+        p.ring = b->d_ring;
+        p.ring_mask = b->ring_mask;
+        p.aq = b->d_aq;
+    }
     block = o.block_size;
     const int bps = blocks_per_sm_for(o, false, o.mapping);
     if (bps <= 0) return set_error(PFG_ERR_CUDA, "occupancy query failed for block size %d", block);
@@ -363,7 +378,12 @@ static pfg_status batch_complete(pfg_batch* b, int mode, u32 delta, pfg_stats* s
         case DS_OK: return PFG_OK;
         case DS_BAD_SOURCE: return set_error(PFG_ERR_INVALID_ARGUMENT, "source out of range");
         case DS_NOT_CONVERGED: return set_error(PFG_ERR_NOT_CONVERGED, "batch did not converge");
-        case DS_TIMEOUT: return set_error(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
+        case DS_TIMEOUT:
+            // the next run must find the ring empty
+            cudaMemsetAsync(b->d_ring, 0xFF, ((u64)b->ring_mask + 1) * 4, b->stream);
+            cudaMemsetAsync(b->d_aq, 0, AQ_WORDS * 4, b->stream);
+            cudaStreamSynchronize(b->stream);
+            return set_error(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
         default: return set_error(PFG_ERR_CUDA, "device status %u", c->rd.status);
     }
 }

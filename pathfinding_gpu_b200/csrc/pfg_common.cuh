@@ -41,8 +41,14 @@ enum Phase : u32 {
     PH_NAIVE = 4,  // Bellman-Ford sweep over all vertices (naive mode)
     PH_COMPACT = 5,// prefix-sum compaction of the flagged next frontier
     PH_DONE = 6,
-    PH_PAUSE = 7   // serving: the step's round budget is spent; Ctl::resume_phase is next
+    PH_PAUSE = 7,  // serving: the step's round budget is spent; Ctl::resume_phase is next
+    PH_ASYNC = 8   // bucket drained without rounds: CTAs pull work from the ring queue
 };
+
+// Ring queue of the asynchronous bucket phase: counters in RunParams::aq, one
+// 128-byte line each (u32 index).
+enum RingCounter : u32 { AQ_HEAD = 0, AQ_TAIL = 32, AQ_DONE = 64, AQ_BUSY = 96, AQ_IDLE = 128, AQ_WORDS = 160 };
+constexpr u32 RING_EMPTY = 0xFFFFFFFFu;  // a free ring slot
 
 // Run modes (reference GpuAlgo, include/gpu_sssp.h:10-14).
 enum RunMode : int { MODE_NAIVE = 0, MODE_FRONTIER = 1, MODE_DELTA = 2 };
@@ -169,6 +175,13 @@ struct RunParams {
     u32 eager_max_items;  // ... only in rounds whose input has at most this many items
     const PolicyNet* net;
     u64 timeout_ns;    // bound on every device-side wait
+    // Asynchronous buckets (ring != nullptr): inside a bucket, vertices claimed
+    // for the window go to a ring of ring_mask + 1 slots (RING_EMPTY when free)
+    // and any CTA pulls them as soon as they are written; the grid barrier runs
+    // once per bucket instead of once per relaxation round.
+    u32* ring;
+    u32 ring_mask;
+    u32* aq;           // ring counters, see RingCounter
 };
 
 // ---------------------------------------------------------------------------
@@ -184,6 +197,16 @@ __device__ __forceinline__ u64 global_timer_ns() {
 __device__ __forceinline__ u64 ld_state(const u64* p) { return __ldcg(p); }
 __device__ __forceinline__ u32 ld_cg(const u32* p) { return __ldcg(p); }
 __device__ __forceinline__ u32 vload(const u32* p) { return *(const volatile u32*)p; }
+__device__ __forceinline__ u32 ld_relaxed(const u32* p) {
+    u32 v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ u32 ld_acquire(const u32* p) {
+    u32 v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ u64 vload64(const u64* p) { return *(const volatile u64*)p; }
 
 __device__ __forceinline__ u32 st_dist(u64 s) { return (u32)(s >> 32); }
@@ -253,6 +276,27 @@ __device__ __forceinline__ void queue_push(u32* q, u32* tail, u32 item) {
     if (lane == leader) base = atomicAdd(tail, (u32)__popc(mask));
     base = __shfl_sync(mask, base, leader);
     q[base + __popc(mask & ((1u << lane) - 1u))] = item;
+}
+
+// Warp-aggregated append to the ring queue. The slot of position i was freed
+// by the consumer of position i - (ring_mask + 1); the compare-and-swap makes
+// a writer that catches up with a slow consumer wait (bounded) instead of
+// overwriting an unread item. Returns false if that wait timed out.
+__device__ __forceinline__ bool ring_push(u32* ring, u32 mask_bits, u32* tail, u32 item, u64 timeout_ns) {
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    u32 base = 0;
+    if (lane == leader) base = atomicAdd(tail, (u32)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    u32* slot = ring + ((base + __popc(mask & ((1u << lane) - 1u))) & mask_bits);
+    if (atomicCAS(slot, RING_EMPTY, item) == RING_EMPTY) return true;
+    const u64 t0 = global_timer_ns();
+    while (atomicCAS(slot, RING_EMPTY, item) != RING_EMPTY) {
+        if (global_timer_ns() - t0 > timeout_ns) return false;
+        __nanosleep(64);
+    }
+    return true;
 }
 
 }  // namespace pfg

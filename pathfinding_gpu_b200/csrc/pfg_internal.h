@@ -36,6 +36,9 @@ u32 eager_rounds_for(const pfg_options& o);
 // as the bound of every device-side wait, in nanoseconds.
 u64 device_timeout_ns();
 
+// Whether a run drains its buckets asynchronously (ring queue + claimed lists).
+bool async_buckets_for(const pfg_options& o, int mode, bool policy, bool traced);
+
 }  // namespace pfg
 
 #include <string>
@@ -67,6 +70,9 @@ struct pfg_solver {
     u32* d_q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // near0, near1, far0, far1, R
     u32* d_stamp[3] = {nullptr, nullptr, nullptr};                // near, far, R
     u32* d_naive[2] = {nullptr, nullptr};
+    u32* d_ring = nullptr;      // ring queue of asynchronous buckets [ring_mask + 1], RING_EMPTY when idle
+    u32 ring_mask = 0;
+    u32* d_aq = nullptr;        // ring counters [AQ_WORDS]
     u32* d_srcs = nullptr;
     u32* d_path = nullptr;      // path extraction scratch [n + 1]
     u32* d_path_len = nullptr;

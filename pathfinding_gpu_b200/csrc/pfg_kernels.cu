@@ -57,8 +57,9 @@ struct Coop {
     u32 inst[MAX_BS];
     u64 ub[MAX_BS];
     u32 wsum[32];
-    u32 cl[CL_CAP];  // near vertices claimed by this CTA in the current round
-    u32 cl_n;        // entries appended (may exceed CL_CAP; the excess went to the global queue)
+    u32 cl[CL_CAP];  // near vertices claimed by this CTA (circular: position i is cl[i % CL_CAP])
+    u32 cl_n;        // positions appended (may run past cl_head + CL_CAP; the excess went to a global queue)
+    u32 cl_head;     // first position not yet taken (rounds: always 0; asynchronous buckets: advances)
     u32 cl_base;
 };
 
@@ -180,10 +181,15 @@ __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32
             L.pushes++;
             if (cl) {
                 const u32 slot = atomicAdd(&cl->cl_n, 1u);
-                if (slot < CL_CAP) {
-                    cl->cl[slot] = gv;
+                if (slot - cl->cl_head < CL_CAP) {
+                    cl->cl[slot & (CL_CAP - 1u)] = gv;
                     return;
                 }
+            }
+            if (p.ring) {
+                if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, gv, p.timeout_ns))
+                    atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                return;
             }
             const u32 out = s.in_buf ^ 1u;
             queue_push(p.nearq[out], &c->cnt[C_NEAR0 + out], gv);
@@ -334,12 +340,42 @@ __device__ __forceinline__ void flush_claimed(const RunParams& p, const Snap& s,
 // ---------------------------------------------------------------------------
 // One round over an input array of items (state indices).
 // ---------------------------------------------------------------------------
+// Relaxes the selected arcs of the items held by the CTA's threads (at most one
+// item per thread) with the mapping MAP. Called by every thread of the CTA.
+template <bool ASTAR, int AM, int MAP>
+__device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, bool act, u32 u, u32 du,
+                                            u32 ib, u64 ub, u32 inst, u32 eb, u32 ee, Local& L, Coop& cs,
+                                            Coop* cl) {
+    if constexpr (MAP == 0) {  // thread per item
+        if (act) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, inst, eb, ee, L);
+    } else if constexpr (MAP == 1) {  // warp per item
+        const u32 lane = threadIdx.x & 31u;
+        unsigned ballot = __ballot_sync(FULL, act);
+        while (ballot) {
+            const int leader = __ffs(ballot) - 1;
+            ballot &= ballot - 1;
+            const u32 wu = __shfl_sync(FULL, u, leader), wdu = __shfl_sync(FULL, du, leader);
+            const u32 wib = __shfl_sync(FULL, ib, leader), winst = __shfl_sync(FULL, inst, leader);
+            const u64 wub = __shfl_sync(FULL, ub, leader);
+            const u32 web = __shfl_sync(FULL, eb, leader), wee = __shfl_sync(FULL, ee, leader);
+            for (u32 e = web + lane; e < wee; e += 32) {
+                const uint2 a = __ldg(p.adj + e);
+                relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, winst, a.x, a.y, L, nullptr);
+            }
+        }
+    } else {
+        relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
+    }
+}
+
 template <bool ASTAR, int AM, int MAP>
 __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u32 count, int kind,
                             Local& L, Coop& cs) {
     const u32 BS = blockDim.x;
     // Hybrid mapping keeps claimed near vertices in shared memory (see relax_arc).
-    Coop* cl = (MAP == 2 && !p.prefix_scan) ? &cs : nullptr;
+    // A heavy round between asynchronous buckets sends them to the ring, which
+    // the drain that follows it empties.
+    Coop* cl = (MAP == 2 && !p.prefix_scan && !(p.ring && kind == K_HEAVY)) ? &cs : nullptr;
     // Every CTA takes one contiguous slice of the input, so a small frontier is
     // spread over all SMs (one arc chain per thread) instead of a few CTAs.
     const u32 per = (count + gridDim.x - 1u) / gridDim.x;
@@ -352,30 +388,10 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
         bool act = false;
         if (idx < send)
             act = take_item<ASTAR>(p, s, ld_cg(in + idx), kind, L, u, ib, du, ub, inst, eb, ee);
-
-        if constexpr (MAP == 0) {  // thread per item
-            if (act) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, inst, eb, ee, L);
-        } else if constexpr (MAP == 1) {  // warp per item
-            const u32 lane = threadIdx.x & 31u;
-            unsigned ballot = __ballot_sync(FULL, act);
-            while (ballot) {
-                const int leader = __ffs(ballot) - 1;
-                ballot &= ballot - 1;
-                const u32 wu = __shfl_sync(FULL, u, leader), wdu = __shfl_sync(FULL, du, leader);
-                const u32 wib = __shfl_sync(FULL, ib, leader), winst = __shfl_sync(FULL, inst, leader);
-                const u64 wub = __shfl_sync(FULL, ub, leader);
-                const u32 web = __shfl_sync(FULL, eb, leader), wee = __shfl_sync(FULL, ee, leader);
-                for (u32 e = web + lane; e < wee; e += 32) {
-                    const uint2 a = __ldg(p.adj + e);
-                    relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, winst, a.x, a.y, L, nullptr);
-                }
-            }
-        } else {
-            relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
-        }
+        relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
     }
     if constexpr (MAP == 2) {
-        if (cl) {
+        if (cl && !p.ring) {  // (asynchronous buckets drain the claimed list themselves)
             // Eager sub-rounds: the vertices this CTA claimed for the next round
             // (keys inside the bucket window) are relaxed again right away, so
             // the wavefront advances several hops per grid barrier. They stay in
@@ -405,6 +421,181 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
             }
             flush_claimed(p, s, cs);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Asynchronous drain of a bucket (phase ASYNC). Each CTA works through its own
+// claimed list first (the near vertices its relaxations claimed, kept in shared
+// memory, up to one block of items per pass), so a wavefront advances hop by
+// hop without any global queue traffic. Work moves between CTAs through the
+// ring: a CTA spills the newest part of its backlog there when other CTAs are
+// idle (or the backlog exceeds half a block), and a CTA with an empty list
+// reserves a chunk of ring positions with a compare-and-swap on the head.
+//
+// Termination: AQ_BUSY counts the CTAs that still scan their slice of the
+// bucket input or hold claimed-list items; AQ_DONE counts ring items relaxed.
+// A CTA with nothing to do leaves once busy == 0 and done == tail: then no CTA
+// holds work and every item ever pushed has been relaxed, so nothing can be
+// pushed any more. A CTA takes a busy unit before it counts the ring chunk that
+// gave it claimed items as done, and returns it only after the pushes of its
+// last pass were performed, so the test never passes while work exists.
+//
+// A popped vertex releases its claim before its state is read (the fence
+// orders the two), so an improvement that lands after the read queues it again.
+// ---------------------------------------------------------------------------
+template <bool ASTAR, int AM, int MAP>
+__device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& cs, bool busy_held) {
+    __shared__ u32 s_src, s_h, s_n, s_spill, s_spill_from, s_spill_base, s_busy, s_idle;
+    constexpr u32 CLM = CL_CAP - 1u;
+    const u32 G = gridDim.x, BS = blockDim.x;
+    u32* aq = p.aq;
+    Ctl* c = p.ctl;
+    if (threadIdx.x == 0) {
+        s_busy = busy_held ? 1u : 0u;
+        s_idle = 0u;
+    }
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // appends past cl_head + CL_CAP went to the ring already
+            u32 tail = cs.cl_n;
+            if ((int)(tail - (cs.cl_head + CL_CAP)) > 0) tail = cs.cl_head + CL_CAP;
+            cs.cl_n = tail;
+            const u32 local = tail - cs.cl_head;
+            u32 src = 0, h = 0, n = 0, spill = 0;
+            if (local > 0u) {
+                src = 1u;
+                h = cs.cl_head;
+                n = local < BS ? local : BS;
+                const u32 backlog = local - n;
+                const u32 keep = BS / 2u;
+                if (backlog >= 32u && (s_idle > 0u || backlog > keep))
+                    spill = s_idle > 0u ? backlog / 2u : backlog - keep;
+                cs.cl_head = h + n;
+            } else {
+                if (s_busy) {  // the last pass's pushes were performed before the barrier above
+                    atomicSub(aq + AQ_BUSY, 1u);
+                    s_busy = 0u;
+                }
+                bool idle = false;
+                const u64 t0 = global_timer_ns();
+                for (u32 spin = 1;; ++spin) {
+                    if ((spin & 15u) == 0u) {
+                        if (vload(&c->rd.status) != DS_OK) break;
+                        if (global_timer_ns() - t0 > p.timeout_ns) {
+                            atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                            break;
+                        }
+                    }
+                    const u32 busy = ld_acquire(aq + AQ_BUSY);
+                    const u32 done = ld_acquire(aq + AQ_DONE);
+                    const u32 t = ld_acquire(aq + AQ_TAIL);
+                    const u32 hh = ld_relaxed(aq + AQ_HEAD);
+                    if ((int)(t - hh) > 0) {
+                        const u32 avail = t - hh;
+                        u32 want = (avail + G - 1u) / G;
+                        want = want < 32u ? 32u : want;
+                        want = want > BS ? BS : want;
+                        want = want > avail ? avail : want;
+                        if (atomicCAS(aq + AQ_HEAD, hh, hh + want) == hh) {
+                            src = 2u;
+                            h = hh;
+                            n = want;
+                            break;
+                        }
+                        continue;  // another CTA took these positions first
+                    }
+                    if (busy == 0u && done == t) break;  // the bucket is drained
+                    if (!idle) {
+                        atomicAdd(aq + AQ_IDLE, 1u);
+                        idle = true;
+                    }
+                    __nanosleep(64);
+                }
+                if (idle) atomicSub(aq + AQ_IDLE, 1u);
+            }
+            s_src = src;
+            s_h = h;
+            s_n = n;
+            s_spill = spill;
+            if (spill) {
+                s_spill_from = tail - spill;
+                s_spill_base = atomicAdd(aq + AQ_TAIL, spill);
+            }
+        }
+        __syncthreads();
+        const u32 src = s_src, h = s_h, n = s_n, spill = s_spill;
+        if (n == 0u) break;  // block-uniform
+        if (spill) {
+            // the newest part of the backlog goes to the ring for idle CTAs
+            const u32 from = s_spill_from, base = s_spill_base;
+            for (u32 i = threadIdx.x; i < spill; i += BS) {
+                u32* slot = p.ring + ((base + i) & p.ring_mask);
+                const u32 gi = cs.cl[(from + i) & CLM];
+                if (atomicCAS(slot, RING_EMPTY, gi) != RING_EMPTY) {
+                    const u64 t0 = global_timer_ns();
+                    while (atomicCAS(slot, RING_EMPTY, gi) != RING_EMPTY) {
+                        if (global_timer_ns() - t0 > p.timeout_ns) {
+                            atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) cs.cl_n = from;
+            __syncthreads();
+        }
+        u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, inst = 0;
+        u64 ub = ~0ull;
+        bool act = false;
+        if (threadIdx.x < n) {
+            u32 gi;
+            if (src == 1u) {
+                gi = cs.cl[(h + threadIdx.x) & CLM];
+            } else {
+                u32* slot = p.ring + ((h + threadIdx.x) & p.ring_mask);
+                gi = ld_relaxed(slot);
+                if (gi == RING_EMPTY) {
+                    // reserved by a producer that has not written it yet
+                    const u64 t0 = global_timer_ns();
+                    while ((gi = ld_relaxed(slot)) == RING_EMPTY) {
+                        if (global_timer_ns() - t0 > p.timeout_ns) {
+                            atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                if (gi != RING_EMPTY) *slot = RING_EMPTY;
+            }
+            if (gi != RING_EMPTY) {
+                p.near_stamp[gi] = 0u;  // release the claim (epochs start at 1)
+                __threadfence();
+                act = take_item<ASTAR>(p, s, gi, K_LIGHT, L, u, ib, du, ub, inst, eb, ee);
+            }
+        }
+        u32 idle_now = 0u;
+        if (threadIdx.x == 0) idle_now = ld_relaxed(aq + AQ_IDLE);
+        relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, MAP == 2 ? &cs : nullptr);
+        __syncthreads();  // every push of the pass has been performed
+        if (threadIdx.x == 0) {
+            s_idle = idle_now;
+            if (src == 2u) {
+                if (cs.cl_n != cs.cl_head && !s_busy) {
+                    atomicAdd(aq + AQ_BUSY, 1u);
+                    s_busy = 1u;
+                    __threadfence();  // busy is raised before the chunk counts as done
+                }
+                atomicAdd(aq + AQ_DONE, n);
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        cs.cl_n = 0u;
+        cs.cl_head = 0u;
     }
 }
 
@@ -596,7 +787,12 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
             for (u32 i = 0; i < p.k && !bad; ++i) {
                 const u32 gi = (p.inst_off ? p.inst_off[i] : i * p.n) + p.srcs[i];
                 p.state[gi] = pack_state(0u, NO_PARENT);
-                if (p.mode != MODE_NAIVE) p.nearq[0][i] = gi;
+                if (p.ring) {
+                    p.ring[i & p.ring_mask] = gi;  // free: every earlier run left the ring empty
+                    p.near_stamp[gi] = r.near_epoch;
+                } else if (p.mode != MODE_NAIVE) {
+                    p.nearq[0][i] = gi;
+                }
             }
             sc.iterations += 1u;
             if (bad) {
@@ -623,6 +819,17 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
                 sc.bucket_near = p.k;
                 sc.bucket_rounds = 0u;
                 r.phase = PH_LIGHT;
+                if (p.ring) {
+                    // the seeds are the ring's first k positions
+                    p.aq[AQ_HEAD] = 0u;
+                    p.aq[AQ_TAIL] = p.k;
+                    p.aq[AQ_DONE] = 0u;
+                    p.aq[AQ_BUSY] = 0u;
+                    p.aq[AQ_IDLE] = 0u;
+                    sc.cnt[C_NEAR0] = 0u;
+                    r.in_count = 0u;
+                    r.phase = PH_ASYNC;
+                }
                 if (p.mode == MODE_DELTA && (p.policy || p.trace)) {
                     // The first bucket is a decision point too: features of the
                     // seed window (nothing relaxed yet) and the graph.
@@ -652,6 +859,15 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
             } else {
                 r.phase = PH_DONE;
             }
+        } else if (ph == PH_ASYNC) {
+            // the ring is drained: light arcs of the window are done
+            sc.iterations += 1u;
+            if (r.heavy && sc.cnt[C_R]) {
+                r.in_count = sc.cnt[C_R];
+                r.phase = PH_HEAVY;
+            } else {
+                advance = true;
+            }
         } else if (ph == PH_LIGHT || ph == PH_SCAN) {
             const u32 nn = sc.cnt[C_NEAR0 + out];
             if (p.prefix_scan) {
@@ -678,7 +894,19 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
             sc.cnt[C_R] = 0u;
             r.r_epoch += 1u;  // R may be refilled in this bucket (A*)
             const u32 nn = sc.cnt[C_NEAR0 + out];
-            if (nn) {
+            if (p.ring) {
+                // asynchronous buckets: heavy arcs that land inside the window
+                // (A* keys) queued their heads in the ring; drain it again
+                if (__ldcg(p.aq + AQ_TAIL) != __ldcg(p.aq + AQ_HEAD)) {
+                    p.aq[AQ_BUSY] = 0u;
+                    p.aq[AQ_IDLE] = 0u;
+                    r.in_count = 0u;
+                    sc.iterations += 1u;
+                    r.phase = PH_ASYNC;
+                } else {
+                    advance = true;
+                }
+            } else if (nn) {
                 sc.cnt[C_NEAR0 + in_buf] = 0u;
                 r.in_buf = out;
                 r.in_count = nn;
@@ -762,6 +990,15 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
             sc.bucket_near = 0u;
             sc.bucket_rounds = 0u;
             r.phase = PH_SCAN;
+            if (p.ring) {
+                // every CTA scans its slice of the far pile, then drains the ring
+                p.aq[AQ_HEAD] = 0u;
+                p.aq[AQ_TAIL] = 0u;
+                p.aq[AQ_DONE] = 0u;
+                p.aq[AQ_BUSY] = r.in_count ? gridDim.x : 0u;
+                p.aq[AQ_IDLE] = 0u;
+                r.phase = PH_ASYNC;
+            }
         }
         // keep the persistent stamp counters in step with the round descriptor
         sc.near_epoch = r.near_epoch;
@@ -863,7 +1100,7 @@ __device__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, Ct
 // The persistent kernel.
 // ---------------------------------------------------------------------------
 template <bool ASTAR, int AM, int MAP>
-__global__ void __launch_bounds__(MAX_BS) k_persistent(const __grid_constant__ RunParams p) {
+__global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p) {
     __shared__ Snap s;
     __shared__ Coop cs;
     __shared__ Ctl sc;
@@ -881,6 +1118,7 @@ __global__ void __launch_bounds__(MAX_BS) k_persistent(const __grid_constant__ R
             uint4* dst = reinterpret_cast<uint4*>(&s);
             for (int i = 0; i < 5; ++i) dst[i] = __ldcg(src + i);
             cs.cl_n = 0;
+            cs.cl_head = 0;
             if (s.status != DS_OK) s.phase = PH_DONE;
         }
         __syncthreads();
@@ -893,6 +1131,7 @@ __global__ void __launch_bounds__(MAX_BS) k_persistent(const __grid_constant__ R
         if (threadIdx.x == 0) {
             s.far_out = 0;
             cs.cl_n = 0;
+            cs.cl_head = 0;
         }
         grid_barrier(p, s, L, red, sc, s_flag, s_feat, act0, act1);
     }
@@ -909,6 +1148,14 @@ __global__ void __launch_bounds__(MAX_BS) k_persistent(const __grid_constant__ R
             round_naive<ASTAR, AM>(p, s, L);
         } else if (ph == PH_COMPACT) {
             round_compact(p, s, cs);
+        } else if (ph == PH_ASYNC) {
+            if (s.in_count) {
+                // bucket start: this CTA's slice of the far pile (in-window items
+                // are relaxed at once, the rest stay far), then the ring
+                round_items<ASTAR, AM, MAP>(p, s, p.farq[s.far_in], s.in_count, K_SCAN, L, cs);
+            }
+            // (the transition gave every CTA a busy unit when there is a slice to scan)
+            async_drain<ASTAR, AM, MAP>(p, s, L, cs, s.in_count != 0u);
         }
         grid_barrier(p, s, L, red, sc, s_flag, s_feat, act0, act1);
     }

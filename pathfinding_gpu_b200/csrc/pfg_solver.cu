@@ -285,6 +285,15 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
         TRY(s->dalloc(&s->d_naive[i], words));
         TRYC(cudaMemsetAsync(s->d_naive[i], 0, words * 4, s->stream));
     }
+    // Ring of the asynchronous buckets: a power of two >= K*n slots, so the
+    // live items (at most one per state word) always fit.
+    u64 ring = 1024;
+    while (ring < Kn) ring <<= 1;
+    TRY(s->dalloc(&s->d_ring, ring));
+    TRYC(cudaMemsetAsync(s->d_ring, 0xFF, ring * 4, s->stream));
+    s->ring_mask = (u32)(ring - 1);
+    TRY(s->dalloc(&s->d_aq, (u64)AQ_WORDS));
+    TRYC(cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, s->stream));
     TRY(s->dalloc(&s->d_srcs, K));
     TRY(s->dalloc(&s->d_path, (u64)n + 1));
     TRY(s->dalloc(&s->d_path_len, 1));
@@ -350,6 +359,7 @@ pfg_options default_options() {
     o.policy = PFG_POLICY_FIXED;
     o.eager = -1;
     o.blocks_per_sm = 0;
+    o.schedule = PFG_SCHEDULE_AUTO;
     return o;
 }
 
@@ -358,6 +368,7 @@ void sanitize_options(pfg_options& o) {
     if (o.block_size < 32 || o.block_size > 1024 || (o.block_size % 32) != 0) o.block_size = 256;
     if (o.mapping < 0 || o.mapping > 2) o.mapping = PFG_MAP_HYBRID;
     if (o.atomic < 0 || o.atomic > 2) o.atomic = PFG_ATOMIC_MIN_RBA;
+    if (o.schedule < 0 || o.schedule > 2) o.schedule = PFG_SCHEDULE_AUTO;
 }
 
 int blocks_per_sm_for(const pfg_options& o, bool astar, int map) {
@@ -376,6 +387,10 @@ u32 eager_rounds_for(const pfg_options& o) {
 }
 
 u64 device_timeout_ns() { return (u64)std::max(1, env_int("PFG_TIMEOUT_MS", 2000)) * 1000000ull; }
+
+bool async_buckets_for(const pfg_options& o, int mode, bool policy, bool traced) {
+    return o.schedule != PFG_SCHEDULE_ROUNDS && mode == MODE_DELTA && !policy && !traced;
+}
 
 }  // namespace pfg
 
@@ -483,6 +498,12 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     p.trace = mode == MODE_DELTA ? d_trace : nullptr;
     p.trace_cap = trace_cap;
     p.timeout_ns = device_timeout_ns();
+    // Asynchronous buckets for fixed-Delta Delta-stepping (see pfg_schedule).
+    if (async_buckets_for(o, mode, p.policy != 0, p.trace != nullptr)) {
+        p.ring = s->d_ring;
+        p.ring_mask = s->ring_mask;
+        p.aq = s->d_aq;
+    }
 
     const int map = mode == MODE_NAIVE ? PFG_MAP_THREAD : o.mapping;
     const int block = o.block_size;
@@ -536,9 +557,11 @@ static pfg_status complete_run(pfg_solver* s, pfg_stats* stats_out) {
     }
     const u32 status = c->rd.status;
     if (status == DS_TIMEOUT) {
-        // A wait gave up: reset the naive masks so the next run starts clean.
+        // A wait gave up: reset the naive masks and the ring so the next run starts clean.
         const u64 words = (u64)s->n / 32 + 1;
         for (int i = 0; i < 2; ++i) cudaMemsetAsync(s->d_naive[i], 0, words * 4, s->stream);
+        cudaMemsetAsync(s->d_ring, 0xFF, ((u64)s->ring_mask + 1) * 4, s->stream);
+        cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, s->stream);
         cudaStreamSynchronize(s->stream);
         return fail(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
     }

@@ -51,6 +51,13 @@ class Policy(IntEnum):
     Learned = 1
 
 
+class Schedule(IntEnum):
+    """How a Delta-stepping bucket is worked off (pfg_schedule in include/pfg.h)."""
+    Auto = 0    # Async for fixed-Delta Delta-stepping, Rounds otherwise
+    Rounds = 1  # relaxation rounds separated by grid barriers (the reference's loop)
+    Async = 2   # one drain per bucket through CTA claimed lists and a ring queue
+
+
 @dataclass
 class GpuOptions:
     algo: GpuAlgo = GpuAlgo.DeltaStep
@@ -63,11 +70,12 @@ class GpuOptions:
     policy: Policy = Policy.Fixed
     eager: int = -1  # Hybrid mapping: eager sub-rounds per grid round (-1 engine default, 0 off)
     blocksPerSM: int = 0  # CTAs of the persistent kernel per SM (0: engine default)
+    schedule: Schedule = Schedule.Auto
 
     def to_c(self) -> N.PfgOptions:
         return N.PfgOptions(int(self.algo), int(self.mapping), int(self.atomic), int(self.delta),
                             int(self.blockSize), int(self.syncEvery), int(self.compaction),
-                            int(self.policy), int(self.eager), int(self.blocksPerSM))
+                            int(self.policy), int(self.eager), int(self.blocksPerSM), int(self.schedule))
 
 
 @dataclass

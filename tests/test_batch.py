@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import pathfinding_gpu_b200 as pf
-from pathfinding_gpu_b200 import GpuAlgo, GpuOptions
+from pathfinding_gpu_b200 import GpuAlgo, GpuOptions, Schedule
 from pathfinding_gpu_b200.batch import GpuBatch
 
 pytestmark = pytest.mark.gpu
@@ -23,13 +23,14 @@ def check_instances(oracle, b, graphs, state):
         assert np.array_equal(p, p_can), (i, gi, s)
 
 
-@pytest.mark.parametrize("algo", [GpuAlgo.DeltaStep, GpuAlgo.Frontier])
-def test_uneven_batch_matches_single_runs(oracle, graphs, algo):
+@pytest.mark.parametrize("algo,schedule", [(GpuAlgo.DeltaStep, Schedule.Rounds), (GpuAlgo.DeltaStep, Schedule.Async),
+                                           (GpuAlgo.Frontier, Schedule.Auto)])
+def test_uneven_batch_matches_single_runs(oracle, graphs, algo, schedule):
     inst = [(0, 0), (0, 899), (0, 450), (1, 5), (2, 17), (2, 900), (3, 3), (1, 696)]
     with GpuBatch(graphs, max_instances=16, max_states=8 * 2000) as b:
         b.set_instances(inst)
         for delta in (0, 5, 200):
-            stats, ms = b.run(GpuOptions(algo=algo, delta=delta))
+            stats, ms = b.run(GpuOptions(algo=algo, delta=delta, schedule=schedule))
             check_instances(oracle, b, graphs, b.state())
             assert stats.rounds > 0 and ms > 0
 

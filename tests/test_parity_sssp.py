@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import pathfinding_gpu_b200 as pf
-from pathfinding_gpu_b200 import GpuAlgo, GpuOptions, Mapping, AtomicMode, Compaction
+from pathfinding_gpu_b200 import GpuAlgo, GpuOptions, Mapping, AtomicMode, Compaction, Schedule
 
 pytestmark = pytest.mark.gpu
 
@@ -66,18 +66,45 @@ def test_grid100_all_sources(oracle, grid100, grid100_solver, algo):
         check_sssp(oracle, grid100, src, res)
 
 
+SCHEDULES = [Schedule.Rounds, Schedule.Async]
+
+
 @pytest.mark.parametrize("mapping,atomic", list(itertools.product(list(Mapping), list(AtomicMode))))
-def test_grid100_variants(oracle, grid100, grid100_solver, mapping, atomic):
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_grid100_variants(oracle, grid100, grid100_solver, mapping, atomic, schedule):
     for algo in (GpuAlgo.DeltaStep, GpuAlgo.Frontier):
-        res = grid100_solver.sssp(77, GpuOptions(algo=algo, mapping=mapping, atomic=atomic))
+        res = grid100_solver.sssp(77, GpuOptions(algo=algo, mapping=mapping, atomic=atomic, schedule=schedule))
         check_sssp(oracle, grid100, 77, res)
 
 
 @pytest.mark.parametrize("delta", [1, 7, 60, 100, 120, 149, 150, 1000, 100000])
-def test_grid100_delta_sweep(oracle, grid100, grid100_solver, delta):
-    res = grid100_solver.sssp(4321, GpuOptions(delta=delta))
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_grid100_delta_sweep(oracle, grid100, grid100_solver, delta, schedule):
+    res = grid100_solver.sssp(4321, GpuOptions(delta=delta, schedule=schedule))
     check_sssp(oracle, grid100, 4321, res)
     assert res.stats.delta == delta
+
+
+def test_async_buckets_take_one_barrier_per_bucket(grid100_solver):
+    # a bucket is one drain: far fewer barrier epochs than relaxation rounds
+    a = grid100_solver.sssp(0, GpuOptions(schedule=Schedule.Async)).stats
+    r = grid100_solver.sssp(0, GpuOptions(schedule=Schedule.Rounds)).stats
+    assert a.rounds <= a.buckets + 2 < r.rounds
+
+
+@pytest.mark.parametrize("block", [32, 256, 1024])
+def test_grid300_async_batch(oracle, block):
+    # wider wavefronts: claimed lists overflow and spill into the ring
+    g = pf.grid(300, 300, SEED)
+    srcs = pf.uniform_vertices(g.n, 8, SEED + 3).tolist()
+    with pf.GpuSolver(g, 8) as s:
+        for atomic in (AtomicMode.MinRBA, AtomicMode.MinNoCheck):
+            _, _, state = s.run_state(srcs, GpuOptions(blockSize=block, atomic=atomic, schedule=Schedule.Async))
+            dist, parent = pf.unpack(state)
+            for i, src in enumerate(srcs):
+                d_ref, p_can = oracle.sssp_canonical(g, src)
+                assert np.array_equal(dist[i * g.n:(i + 1) * g.n], d_ref), (block, atomic, i)
+                assert np.array_equal(parent[i * g.n:(i + 1) * g.n], p_can), (block, atomic, i)
 
 
 @pytest.mark.parametrize("eager", [0, 1, 3, 16, 64])
@@ -118,12 +145,17 @@ def test_grid100_astar(oracle, grid100, grid100_solver):
             r = grid100_solver.astar(s, t, GpuOptions(algo=algo))
             assert r.targetDist == d_ref[t], (s, t, algo)
             assert oracle.validate_path(grid100, r.path, s, t, int(d_ref[t])), (s, t, algo)
+        for schedule, delta in itertools.product(SCHEDULES, (0, 60)):
+            r = grid100_solver.astar(s, t, GpuOptions(schedule=schedule, delta=delta))
+            assert r.targetDist == d_ref[t], (s, t, schedule, delta)
+            assert oracle.validate_path(grid100, r.path, s, t, int(d_ref[t])), (s, t, schedule, delta)
 
 
-def test_grid100_multisource(oracle, grid100, grid100_solver):
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_grid100_multisource(oracle, grid100, grid100_solver, schedule):
     srcs = sources_c0(grid100)
     for algo in (GpuAlgo.DeltaStep, GpuAlgo.Frontier):
-        stats, ms, state = grid100_solver.run_state(srcs, GpuOptions(algo=algo))
+        stats, ms, state = grid100_solver.run_state(srcs, GpuOptions(algo=algo, schedule=schedule))
         dist, parent = pf.unpack(state)
         dist = dist.reshape(len(srcs), -1)
         parent = parent.reshape(len(srcs), -1)
@@ -141,11 +173,13 @@ def test_rmat_variants(oracle, rmat12, rmat12_solver):
             check_sssp(oracle, rmat12, int(s), res)
 
 
-def test_rmat_small_delta_heavy_phase(oracle, rmat12, rmat12_solver):
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_rmat_small_delta_heavy_phase(oracle, rmat12, rmat12_solver, schedule):
     # Delta below the max weight exercises the R set and heavy rounds
+    src = int(pf.pick_sources(rmat12, 1, 7)[0])
     for delta in (1, 16, 64, 200):
-        res = rmat12_solver.sssp(int(pf.pick_sources(rmat12, 1, 7)[0]), GpuOptions(delta=delta))
-        check_sssp(oracle, rmat12, int(pf.pick_sources(rmat12, 1, 7)[0]), res)
+        res = rmat12_solver.sssp(src, GpuOptions(delta=delta, schedule=schedule))
+        check_sssp(oracle, rmat12, src, res)
         assert res.stats.buckets >= 1
 
 
