@@ -66,8 +66,8 @@ enum pfg_policy_kind { PFG_POLICY_FIXED = 0, PFG_POLICY_LEARNED = 1 };
  * ASYNC:  one drain per bucket: CTAs relax the vertices they claim from their
  *         own shared-memory list and share work through a ring queue, with a
  *         grid barrier only between buckets.
- * AUTO:   ASYNC for fixed-Delta Delta-stepping, ROUNDS otherwise (Naive,
- *         Frontier, learned policy, traced runs, serving steps). */
+ * AUTO:   ASYNC for Delta-stepping, ROUNDS for Naive and Frontier (serving
+ *         steps always run rounds: a step is bounded by a number of rounds). */
 enum pfg_schedule { PFG_SCHEDULE_AUTO = 0, PFG_SCHEDULE_ROUNDS = 1, PFG_SCHEDULE_ASYNC = 2 };
 
 /* Mirrors GpuOptions (reference: include/gpu_sssp.h:42-52) plus `policy`. */
@@ -86,7 +86,7 @@ typedef struct pfg_options {
     int32_t blocks_per_sm; /* CTAs of the persistent kernel per SM; 0 = engine
                               default (1024 resident threads per SM) (extension) */
     int32_t schedule;    /* enum pfg_schedule, default PFG_SCHEDULE_AUTO; ASYNC
-                            applies to fixed-Delta runs only (extension)        */
+                            applies to Delta-stepping only (extension)          */
 } pfg_options;
 
 /* Mirrors GpuStats (reference: include/gpu_sssp.h:55-65) plus `rounds`. */

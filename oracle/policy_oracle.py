@@ -1,17 +1,17 @@
 """ORACLE - test infrastructure only.
 
-fp64 numpy restatement of the learned Delta policy network (12 -> 64 -> 64 -> 64 -> 8,
+fp64 numpy restatement of the learned Delta policy network (12 -> 64 -> 64 -> 64 -> 16,
 ReLU, softmax cross-entropy against soft targets), its gradient, and a
 finite-difference check of that gradient. The network has no counterpart in the
 reference; the CUDA kernels of pathfinding_gpu_b200/csrc/pfg_policy.cu are checked
 against this file. Parameter layout (flat float32 image): w1[64x12] b1[64]
-w2[64x64] b2[64] w3[64x64] b3[64] w4[8x64] b4[8] in_mean[12] in_scale[12].
+w2[64x64] b2[64] w3[64x64] b3[64] w4[16x64] b4[16] in_mean[12] in_scale[12].
 """
 from __future__ import annotations
 
 import numpy as np
 
-IN, H, OUT = 12, 64, 8
+IN, H, OUT = 12, 64, 16
 SIZES = [("w1", (H, IN)), ("b1", (H,)), ("w2", (H, H)), ("b2", (H,)), ("w3", (H, H)), ("b3", (H,)),
          ("w4", (OUT, H)), ("b4", (OUT,)), ("in_mean", (IN,)), ("in_scale", (IN,))]
 NP = sum(int(np.prod(s)) for _, s in SIZES)

@@ -327,7 +327,7 @@ static pfg_status batch_prepare(pfg_batch* b, const pfg_options* opt_in, RunPara
     p.eager = eager_rounds_for(o);
     if (o.eager < 0 && b->avg_deg > 6.0) p.eager = 0;  // as the single-graph solver: road-like graphs only
     p.timeout_ns = device_timeout_ns();
-    if (async_buckets_for(o, mode, false, false)) {
+    if (async_buckets_for(o, mode)) {
         p.ring = b->d_ring;
         p.ring_mask = b->ring_mask;
         p.aq = b->d_aq;

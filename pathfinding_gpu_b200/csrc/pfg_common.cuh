@@ -65,7 +65,9 @@ struct __align__(16) Rd {
     u32 phase, in_count, in_buf, far_in;   // input of the round
     u32 far_out, status, delta, heavy;     // far pile receiving pushes, Delta of the bucket
     u32 near_epoch, far_epoch, r_epoch, naive_in;  // dedup stamps of this round's outputs
-    u32 flag_epoch, map_mode, pad0, pad1;
+    u32 flag_epoch, map_mode;
+    u32 async_bkt;                         // 1: this bucket is drained asynchronously (ring + claimed lists)
+    u32 in_kind;                           // ASYNC input slice: 0 far pile, 1 near queue (the seeds)
     u64 lo, hi;                            // bucket window [lo, hi) on the key
 };
 
@@ -108,7 +110,7 @@ static_assert(sizeof(Rd) == 80, "Rd layout");
 // Learned Delta-policy network (3 hidden layers of 64, fp32).
 constexpr int POL_IN = 12;
 constexpr int POL_H = 64;
-constexpr int POL_OUT = 8;  // Delta multipliers, see kPolicyMult
+constexpr int POL_OUT = 16; // classes: schedule (c / 8: 0 async, 1 rounds) x Delta multiplier kPolicyMult[c % 8]
 constexpr int TRACE_W = 16; // trace row: POL_IN features, then bucket index, Delta, items, rounds
 struct PolicyNet {
     float w1[POL_H * POL_IN], b1[POL_H];

@@ -37,7 +37,7 @@ u32 eager_rounds_for(const pfg_options& o);
 u64 device_timeout_ns();
 
 // Whether a run drains its buckets asynchronously (ring queue + claimed lists).
-bool async_buckets_for(const pfg_options& o, int mode, bool policy, bool traced);
+bool async_buckets_for(const pfg_options& o, int mode);
 
 }  // namespace pfg
 

@@ -33,8 +33,9 @@ constexpr u32 COOP_MIN = 32;  // hybrid mapping: rows with >= 32 selected arcs a
 
 enum Kind { K_LIGHT = 0, K_SCAN = 1, K_HEAVY = 2 };
 
-// Multipliers of the automatic Delta that the learned policy chooses from.
-__constant__ float kPolicyMult[POL_OUT] = {0.25f, 0.5f, 1.f, 2.f, 4.f, 8.f, 16.f, 64.f};
+// Multipliers of the automatic Delta that the learned policy chooses from
+// (class c: multiplier kPolicyMult[c % 8], asynchronous bucket if c < 8).
+__constant__ float kPolicyMult[8] = {0.0625f, 0.125f, 0.25f, 0.5f, 1.f, 2.f, 4.f, 8.f};
 
 // The round descriptor, copied to shared memory after every barrier.
 typedef Rd Snap;
@@ -186,7 +187,7 @@ __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32
                     return;
                 }
             }
-            if (p.ring) {
+            if (s.async_bkt) {
                 if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, gv, p.timeout_ns))
                     atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
                 return;
@@ -375,7 +376,7 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
     // Hybrid mapping keeps claimed near vertices in shared memory (see relax_arc).
     // A heavy round between asynchronous buckets sends them to the ring, which
     // the drain that follows it empties.
-    Coop* cl = (MAP == 2 && !p.prefix_scan && !(p.ring && kind == K_HEAVY)) ? &cs : nullptr;
+    Coop* cl = (MAP == 2 && !p.prefix_scan && !(s.async_bkt && kind == K_HEAVY)) ? &cs : nullptr;
     // Every CTA takes one contiguous slice of the input, so a small frontier is
     // spread over all SMs (one arc chain per thread) instead of a few CTAs.
     const u32 per = (count + gridDim.x - 1u) / gridDim.x;
@@ -391,7 +392,7 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
         relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
     }
     if constexpr (MAP == 2) {
-        if (cl && !p.ring) {  // (asynchronous buckets drain the claimed list themselves)
+        if (cl && !s.async_bkt) {  // (asynchronous buckets drain the claimed list themselves)
             // Eager sub-rounds: the vertices this CTA claimed for the next round
             // (keys inside the bucket window) are relaxed again right away, so
             // the wavefront advances several hops per grid barrier. They stay in
@@ -751,6 +752,26 @@ __device__ void decision_features(const RunParams& p, Ctl& sc, const Rd& r, u32 
     }
 }
 
+// Turns the bucket that starts now into an asynchronous one: every CTA scans
+// its slice of the input (the far pile, or with from_near the seeds in near
+// queue 0) and then drains the ring and its claimed list. Run by the
+// transition thread while every other CTA waits at the barrier.
+__device__ __forceinline__ void enter_async(const RunParams& p, Ctl& sc, Rd& r, u32 from_near) {
+    p.aq[AQ_HEAD] = 0u;
+    p.aq[AQ_TAIL] = 0u;
+    p.aq[AQ_DONE] = 0u;
+    p.aq[AQ_BUSY] = r.in_count ? gridDim.x : 0u;
+    p.aq[AQ_IDLE] = 0u;
+    if (from_near) {
+        r.in_buf = 0u;
+        sc.cnt[C_NEAR0] = 0u;  // the slice length travels in r.in_count
+        sc.cnt[C_NEAR1] = 0u;
+    }
+    r.in_kind = from_near;
+    r.async_bkt = 1u;
+    r.phase = PH_ASYNC;
+}
+
 __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_feat, float* act0,
                            float* act1) {
     const u32 t = threadIdx.x;
@@ -787,12 +808,7 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
             for (u32 i = 0; i < p.k && !bad; ++i) {
                 const u32 gi = (p.inst_off ? p.inst_off[i] : i * p.n) + p.srcs[i];
                 p.state[gi] = pack_state(0u, NO_PARENT);
-                if (p.ring) {
-                    p.ring[i & p.ring_mask] = gi;  // free: every earlier run left the ring empty
-                    p.near_stamp[gi] = r.near_epoch;
-                } else if (p.mode != MODE_NAIVE) {
-                    p.nearq[0][i] = gi;
-                }
+                if (p.mode != MODE_NAIVE) p.nearq[0][i] = gi;
             }
             sc.iterations += 1u;
             if (bad) {
@@ -819,17 +835,8 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
                 sc.bucket_near = p.k;
                 sc.bucket_rounds = 0u;
                 r.phase = PH_LIGHT;
-                if (p.ring) {
-                    // the seeds are the ring's first k positions
-                    p.aq[AQ_HEAD] = 0u;
-                    p.aq[AQ_TAIL] = p.k;
-                    p.aq[AQ_DONE] = 0u;
-                    p.aq[AQ_BUSY] = 0u;
-                    p.aq[AQ_IDLE] = 0u;
-                    sc.cnt[C_NEAR0] = 0u;
-                    r.in_count = 0u;
-                    r.phase = PH_ASYNC;
-                }
+                r.async_bkt = 0u;
+                if (p.ring && !(p.mode == MODE_DELTA && p.policy)) enter_async(p, sc, r, 1u);
                 if (p.mode == MODE_DELTA && (p.policy || p.trace)) {
                     // The first bucket is a decision point too: features of the
                     // seed window (nothing relaxed yet) and the graph.
@@ -894,7 +901,7 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
             sc.cnt[C_R] = 0u;
             r.r_epoch += 1u;  // R may be refilled in this bucket (A*)
             const u32 nn = sc.cnt[C_NEAR0 + out];
-            if (p.ring) {
+            if (r.async_bkt) {
                 // asynchronous buckets: heavy arcs that land inside the window
                 // (A* keys) queued their heads in the ring; drain it again
                 if (__ldcg(p.aq + AQ_TAIL) != __ldcg(p.aq + AQ_HEAD)) {
@@ -957,19 +964,20 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
     if (t == 0) {
         Rd& r = sc.rd;
         if (need == 3u) {
-            // first bucket under the policy: window [key0, key0 + Delta)
-            const float dm = (float)p.delta * kPolicyMult[s_flag[1]];
+            // first bucket under the policy: the aligned window holding key0
+            const float dm = (float)p.delta * kPolicyMult[s_flag[1] & 7u];
             const u32 d = dm < 1.f ? 1u : (dm > 2.0e9f ? 2000000000u : (u32)dm);
             r.delta = d;
             r.heavy = d < p.maxw ? 1u : 0u;
-            r.hi = s_key0 + d;
+            r.hi = (s_key0 / d + 1ull) * d;  // aligned, as a fixed-Delta run's first window
             sc.policy_calls += 1u;
+            if (p.ring && s_flag[1] < 8u) enter_async(p, sc, r, 1u);
         } else if (need != 0u) {
             // Open the next bucket: the far pile collected during this bucket is
             // scanned against the window [old hi, new hi).
             u32 d = p.delta;
             if (need == 1u) {
-                const float dm = (float)p.delta * kPolicyMult[s_flag[1]];
+                const float dm = (float)p.delta * kPolicyMult[s_flag[1] & 7u];
                 d = dm < 1.f ? 1u : (dm > 2.0e9f ? 2000000000u : (u32)dm);
                 sc.policy_calls += 1u;
             }
@@ -978,7 +986,9 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
             r.delta = d;
             r.heavy = d < p.maxw ? 1u : 0u;
             r.lo = r.hi;
-            r.hi = need == 1u ? est + d : (est / d + 1ull) * d;
+            // aligned windows: a policy that keeps choosing class c runs exactly
+            // the buckets of fixed Delta = MULTIPLIERS[c] x the automatic Delta
+            r.hi = (est / d + 1ull) * d;
             r.far_in = fin;
             r.far_out = fin ^ 1u;
             sc.cnt[C_FAR0 + (fin ^ 1u)] = 0u;
@@ -987,17 +997,13 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
             r.r_epoch += 1u;
             r.in_count = sc.cnt[C_FAR0 + fin];
             sc.iterations += 1u;
-            sc.bucket_near = 0u;
             sc.bucket_rounds = 0u;
             r.phase = PH_SCAN;
-            if (p.ring) {
-                // every CTA scans its slice of the far pile, then drains the ring
-                p.aq[AQ_HEAD] = 0u;
-                p.aq[AQ_TAIL] = 0u;
-                p.aq[AQ_DONE] = 0u;
-                p.aq[AQ_BUSY] = r.in_count ? gridDim.x : 0u;
-                p.aq[AQ_IDLE] = 0u;
-                r.phase = PH_ASYNC;
+            r.async_bkt = 0u;
+            sc.bucket_near = 0u;  // (rounds add their near pushes to it)
+            if (p.ring && (need != 1u || s_flag[1] < 8u)) {
+                enter_async(p, sc, r, 0u);
+                sc.bucket_near = r.in_count;
             }
         }
         // keep the persistent stamp counters in step with the round descriptor
@@ -1151,8 +1157,11 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
         } else if (ph == PH_ASYNC) {
             if (s.in_count) {
                 // bucket start: this CTA's slice of the far pile (in-window items
-                // are relaxed at once, the rest stay far), then the ring
-                round_items<ASTAR, AM, MAP>(p, s, p.farq[s.far_in], s.in_count, K_SCAN, L, cs);
+                // are relaxed at once, the rest stay far) or of the seeds
+                if (s.in_kind)
+                    round_items<ASTAR, AM, MAP>(p, s, p.nearq[s.in_buf], s.in_count, K_LIGHT, L, cs);
+                else
+                    round_items<ASTAR, AM, MAP>(p, s, p.farq[s.far_in], s.in_count, K_SCAN, L, cs);
             }
             // (the transition gave every CTA a busy unit when there is a slice to scan)
             async_drain<ASTAR, AM, MAP>(p, s, L, cs, s.in_count != 0u);

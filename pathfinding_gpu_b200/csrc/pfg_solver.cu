@@ -388,8 +388,8 @@ u32 eager_rounds_for(const pfg_options& o) {
 
 u64 device_timeout_ns() { return (u64)std::max(1, env_int("PFG_TIMEOUT_MS", 2000)) * 1000000ull; }
 
-bool async_buckets_for(const pfg_options& o, int mode, bool policy, bool traced) {
-    return o.schedule != PFG_SCHEDULE_ROUNDS && mode == MODE_DELTA && !policy && !traced;
+bool async_buckets_for(const pfg_options& o, int mode) {
+    return o.schedule != PFG_SCHEDULE_ROUNDS && mode == MODE_DELTA;
 }
 
 }  // namespace pfg
@@ -498,8 +498,8 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     p.trace = mode == MODE_DELTA ? d_trace : nullptr;
     p.trace_cap = trace_cap;
     p.timeout_ns = device_timeout_ns();
-    // Asynchronous buckets for fixed-Delta Delta-stepping (see pfg_schedule).
-    if (async_buckets_for(o, mode, p.policy != 0, p.trace != nullptr)) {
+    // Asynchronous buckets for Delta-stepping (see pfg_schedule).
+    if (async_buckets_for(o, mode)) {
         p.ring = s->d_ring;
         p.ring_mask = s->ring_mask;
         p.aq = s->d_aq;

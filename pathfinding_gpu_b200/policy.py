@@ -3,15 +3,16 @@
 At every decision point of Delta-stepping (the first bucket and every bucket
 advance) the persistent kernel computes 12 features of the frontier and the
 graph (see decision_features in pfg_kernels.cu) and, with the policy loaded,
-evaluates a 12 -> 64 -> 64 -> 64 -> 8 MLP whose argmax picks the next bucket's
-Delta as MULTIPLIERS[c] x the automatic Delta. The policy changes the schedule
-only; distances and parents are identical to the fixed-Delta run.
+evaluates a 12 -> 64 -> 64 -> 64 -> 16 MLP whose argmax c picks how the next
+bucket runs: Delta = MULTIPLIERS[c % 8] x the automatic Delta, drained
+asynchronously (c < 8) or in relaxation rounds (c >= 8). The policy changes the
+schedule only; distances and parents are identical to the fixed-Delta run.
 
 Training data comes from the solver itself: for each (graph, source) of the
-synthetic families, fixed-Delta runs at every multiplier are timed and traced;
-every trace row of those runs gets the same soft target, a softmax of the
-negative relative run times, so the network learns which Delta class wins from
-what the frontier looks like.
+synthetic families, fixed-Delta runs of every class (schedule x multiplier) are
+timed and traced; every trace row of a graph gets the same soft target, a
+softmax of the negative relative run times, so the network learns which class
+wins from what the frontier and the graph look like.
 """
 from __future__ import annotations
 
@@ -23,11 +24,18 @@ from typing import Iterable, List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import _native as N
-from .solver import GpuOptions, GpuSolver, Policy
+from .solver import GpuOptions, GpuSolver, Policy, Schedule
 
-IN, H, OUT = 12, 64, 8
+IN, H, OUT = 12, 64, 16
 TRACE_W = 16
-MULTIPLIERS = [0.25, 0.5, 1.0, 2.0, 4.0, 8.0, 16.0, 64.0]
+MULTIPLIERS = [0.0625, 0.125, 0.25, 0.5, 1.0, 2.0, 4.0, 8.0]
+# class c -> (schedule, multiplier); the kernel decodes c the same way
+CLASSES = [(Schedule.Async, m) for m in MULTIPLIERS] + [(Schedule.Rounds, m) for m in MULTIPLIERS]
+
+
+def class_name(c: int) -> str:
+    sch, m = CLASSES[c]
+    return f"{sch.name.lower()}x{m:g}"
 SIZES = [("w1", (H, IN)), ("b1", (H,)), ("w2", (H, H)), ("b2", (H,)), ("w3", (H, H)), ("b3", (H,)),
          ("w4", (OUT, H)), ("b4", (OUT,)), ("in_mean", (IN,)), ("in_scale", (IN,))]
 NP = sum(int(np.prod(s)) for _, s in SIZES)
@@ -119,16 +127,21 @@ def run_traced(solver: GpuSolver, src: int, opt: GpuOptions, cap: int = 4096):
 
 def collect(solver: GpuSolver, sources: Iterable[int], reps: int = 3, rows_per_run: int = 96,
             base: Optional[GpuOptions] = None, seed: int = 0):
-    """Traces and soft targets from fixed-Delta sweeps over MULTIPLIERS."""
+    """Traces and soft targets from fixed-Delta sweeps over CLASSES.
+
+    Each source's sweep is normalised by its fastest multiplier and the curves of
+    all sources of the graph are averaged; every trace row of the graph gets the
+    soft target of that mean curve (one label per graph family, so run-to-run
+    noise of a single source does not flip the class)."""
     rng = np.random.default_rng(seed)
     base = base or GpuOptions()
     auto = solver.autoDelta()
-    X, Y, table = [], [], []
+    traces, curves, table = [], [], []
     for src in sources:
-        times, traces = [], []
-        for mult in MULTIPLIERS:
-            d = max(1, int(round(auto * mult)))
-            o = GpuOptions(**{**base.__dict__, "delta": d, "policy": Policy.Fixed})
+        times = []
+        for sched, mult in CLASSES:
+            d = max(1, int(auto * mult))  # the kernel truncates the same product
+            o = GpuOptions(**{**base.__dict__, "delta": d, "policy": Policy.Fixed, "schedule": sched})
             solver.run_state([src], o, copy=False)  # warm
             ts = []
             tr = None
@@ -140,13 +153,14 @@ def collect(solver: GpuSolver, sources: Iterable[int], reps: int = 3, rows_per_r
             if len(tr) > rows_per_run:
                 tr = tr[np.sort(rng.choice(len(tr), rows_per_run, replace=False))]
             traces.append(tr)
-        y = soft_targets(times)
-        for tr in traces:
-            X.append(tr[:, :IN])
-            Y.append(np.repeat(y[None, :], len(tr), axis=0))
+        curves.append(np.asarray(times) / min(times))
         table.append({"src": int(src), "times_ms": [round(t, 4) for t in times],
-                      "best": MULTIPLIERS[int(np.argmin(times))]})
-    return np.concatenate(X), np.concatenate(Y), table
+                      "best": class_name(int(np.argmin(times)))})
+    mean_curve = np.mean(curves, axis=0)
+    y = soft_targets(mean_curve)
+    X = np.concatenate([tr[:, :IN] for tr in traces])
+    Y = np.repeat(y[None, :], len(X), axis=0)
+    return X, Y, table, [round(float(c), 4) for c in mean_curve]
 
 
 def save(params: np.ndarray, path: Path = WEIGHTS, meta: Optional[dict] = None) -> None:

@@ -2,9 +2,11 @@
 
     python -m pathfinding_gpu_b200.train_policy [--out policy_weights.npz] [--report report.json]
 
-1. Traces: for every (graph, source) of the training families (R-MAT scales 15-18
-   with two weight ranges, grids of 256-768 per side, a road-like grid), fixed-Delta
-   runs at each multiplier of policy.MULTIPLIERS are timed and traced.
+1. Traces: for every (graph, source) of the training families (R-MAT scales 18-20
+   with two edge factors and two weight ranges, seeds other than the evaluation
+   graph's; grids of 256-768 per side; a road-like grid), fixed-Delta
+   runs of each class of policy.CLASSES (schedule x multiplier) are timed and
+   traced.
 2. Training: full-batch Adam with the hand-written kernels of pfg_policy.cu.
 3. Evaluation on graphs NOT used for training (R-MAT scale 20, edge factor 16;
    the 1000 x 1000 grid): learned vs fixed automatic Delta, same sources, results
@@ -26,19 +28,19 @@ from . import policy as P
 from .solver import GpuOptions, GpuSolver, Policy, unpack
 
 TRAIN_FAMILIES = [
-    ("rmat_s15_ef16_w255", lambda: G.rmat(15, 16, w_lo=1, w_hi=255, seed=11)),
-    ("rmat_s16_ef16_w255", lambda: G.rmat(16, 16, w_lo=1, w_hi=255, seed=12)),
-    ("rmat_s17_ef8_w255", lambda: G.rmat(17, 8, w_lo=1, w_hi=255, seed=13)),
-    ("rmat_s16_ef16_w1000", lambda: G.rmat(16, 16, w_lo=1, w_hi=1000, seed=14)),
     ("rmat_s18_ef16_w255", lambda: G.rmat(18, 16, w_lo=1, w_hi=255, seed=15)),
+    ("rmat_s19_ef16_w255", lambda: G.rmat(19, 16, w_lo=1, w_hi=255, seed=16)),
+    ("rmat_s19_ef8_w1000", lambda: G.rmat(19, 8, w_lo=1, w_hi=1000, seed=17)),
+    ("rmat_s20_ef8_w255", lambda: G.rmat(20, 8, w_lo=1, w_hi=255, seed=18)),
+    ("rmat_s20_ef16_w255_seed31", lambda: G.rmat(20, 16, w_lo=1, w_hi=255, seed=31)),
     ("grid_256", lambda: G.grid(256, 256, 21)),
     ("grid_512", lambda: G.grid(512, 512, 22)),
     ("grid_768", lambda: G.grid(768, 768, 23)),
     ("road_512", lambda: G.road(512, seed=24)),
 ]
 EVAL = [
-    ("rmat_s20_ef16 (c2)", lambda: G.rmat(20, 16, seed=2026)),
-    ("grid_1000 (c1)", lambda: G.grid(1000, 1000, 2026)),
+    ("rmat_s20_ef16_seed2026", lambda: G.rmat(20, 16, seed=2026)),
+    ("grid_1000_seed2026", lambda: G.grid(1000, 1000, 2026)),
 ]
 
 
@@ -63,11 +65,13 @@ def main(argv=None):
         g = make()
         with GpuSolver(g, 1) as s:
             srcs = G.pick_sources(g, args.sources, 7).tolist()
-            X, Y, table = P.collect(s, srcs, base=base)
+            X, Y, table, curve = P.collect(s, srcs, base=base, reps=5)
         Xs.append(X)
         Ys.append(Y)
-        report["families"][name] = {"n": g.n, "m": g.m, "rows": len(X), "sweeps": table}
-        print(f"[traces] {name}: {len(X)} rows, best multipliers {[t['best'] for t in table]}", flush=True)
+        report["families"][name] = {"n": g.n, "m": g.m, "rows": len(X), "sweeps": table, "mean_curve": curve}
+        best = P.class_name(int(np.argmin(curve)))
+        print(f"[traces] {name}: {len(X)} rows, best per source {[t['best'] for t in table]}, "
+              f"family label {best}", flush=True)
     X = np.concatenate(Xs)
     Y = np.concatenate(Ys)
     params, losses = P.train(X, Y, steps=args.steps, lr=args.lr)
@@ -90,9 +94,12 @@ def main(argv=None):
                 tl = timed(s, src, learned)
                 _, _, a = s.run_state([src], fixed)
                 sl, _, b = s.run_state([src], learned)
+                _, _, tr = P.run_traced(s, src, learned)
                 rows.append({"src": src, "fixed_ms": round(tf, 4), "learned_ms": round(tl, 4),
                              "speedup": round(tf / tl, 3), "bit_exact": bool(np.array_equal(a, b)),
-                             "learned_buckets": sl.buckets})
+                             "learned_buckets": sl.buckets,
+                             "learned_deltas": [int(x) for x in tr[:, P.IN + 1]],
+                             "learned_rounds_per_bucket": [int(x) for x in tr[:, P.IN + 3]]})
             report["eval"][name] = rows
             sp = statistics.median(r["speedup"] for r in rows)
             print(f"[eval] {name}: median speedup {sp:.2f}x, bit-exact {all(r['bit_exact'] for r in rows)}", flush=True)
