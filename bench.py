@@ -3,9 +3,10 @@
 One step = one multi-source SSSP launch (reference GpuSolver::multiSource,
 src/gpu_sssp.cu:553-569): K sources on the 1000x1000 grid (n = 10^6,
 m = 3,996,000 arcs, w = llround(100 * U[1, 1.5)), seed 2026) relaxed by one
-persistent kernel, fixed automatic Delta. Metric: GTEPS = reachable arcs of all
-K instances / step time (the reference's TEPS definition, src/main.cpp:209-213,
-aggregated over the batch).
+persistent kernel, fixed automatic Delta, buckets drained asynchronously (the
+engine's default schedule). Metric: GTEPS = reachable arcs of all K instances /
+step time (the reference's TEPS definition, src/main.cpp:209-213, aggregated
+over the batch).
 
   value  device time of the step with the graph, sources and working set resident
          in HBM (CUDA events on the solver's stream, L2 flushed between steps)
@@ -14,6 +15,11 @@ aggregated over the batch).
          words into pinned memory, timed on the device
   --impl reference   the reference's own cpuMultiSource (OpenMP, every host thread)
          on the same graph and sources, compiled from its sources into oracle/_ref
+  extras (N = 1, skipped with --no-extras): single-source Delta / Frontier / Naive and
+         256 A* pairs on the same grid; R-MAT-20 learned policy vs fixed Delta;
+         the uneven batch (64 sources on a 1024x1024 grid + 256 grids of 32..316 per
+         side) in one launch replayed from a CUDA graph; A* serving on the
+         2048x2048 road-like graph under Poisson arrivals (p50 / p99 latency).
 
 Multi-GPU: replicas (each rank runs its own batch of sources; no collective on the
 data path), value = all ranks' arcs / max step time over ranks.
@@ -38,6 +44,12 @@ sys.path.insert(0, str(ROOT))
 GRID_SIDE = 1000
 SEED = 2026
 BATCH = 64
+
+
+def HEADLINE_OPTIONS():
+    """Fixed automatic Delta, default schedule (asynchronous buckets), blind atomicMin."""
+    from pathfinding_gpu_b200 import GpuOptions, AtomicMode
+    return GpuOptions(atomic=AtomicMode.MinNoCheck)
 
 
 def parse():
@@ -167,7 +179,7 @@ def run_ours(args, D):
     K = args.batch
     solver = pf.GpuSolver(g, K, device=D.local)
     stream = torch.cuda.ExternalStream(solver.stream(), device=D.local)
-    opt = GpuOptions()
+    opt = HEADLINE_OPTIONS()
     lib = solver._lib
     import ctypes as C
     from pathfinding_gpu_b200 import _native as N
@@ -254,7 +266,8 @@ def run_ours(args, D):
                    "graph": f"grid {GRID_SIDE}x{GRID_SIDE}, 4-neighbour arcs both ways, "
                             f"w=llround(100*U[1,1.5)), seed {SEED}",
                    "n": g.n, "m": g.m, "batch": K, "delta": stats0.delta, "algo": "DeltaStep",
-                   "mapping": "Hybrid", "atomic": "MinRBA", "l2": "flushed between steps (256 MB write)",
+                   "schedule": opt.schedule.name, "mapping": opt.mapping.name, "atomic": opt.atomic.name,
+                   "block": opt.blockSize, "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"replicas x{D.world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 5), "traffic": traffic,
@@ -295,25 +308,77 @@ def cpu_baseline(g, srcs, sample: int):
             "sample": f"{len(srcs)} of the step's sources, cpuMultiSource OpenMP x{threads}"}
 
 
+def _median_ms(fn, reps=5):
+    fn()
+    return statistics.median(fn() for _ in range(reps))
+
+
 def extras(g):
-    """Single-source modes and A* pairs on the same graph (reported beside the headline)."""
+    """The other workloads, timed on the device (reported beside the headline)."""
     import pathfinding_gpu_b200 as pf
-    from pathfinding_gpu_b200 import GpuOptions, GpuAlgo
-    s = pf.GpuSolver(g, 1)
+    from pathfinding_gpu_b200 import GpuOptions, GpuAlgo, Policy
     out = {}
-    src = int(pf.uniform_vertices(g.n, 1, SEED)[0])
-    for algo in (GpuAlgo.DeltaStep, GpuAlgo.Frontier, GpuAlgo.NaiveRelax):
-        s.run_state([src], GpuOptions(algo=algo), copy=False)
-        ts = [s.run_state([src], GpuOptions(algo=algo), copy=False)[1] for _ in range(3)]
-        out[f"sssp_{algo.name}_ms"] = round(statistics.median(ts), 3)
-    pairs = pf.uniform_vertices(g.n, 2 * 32, SEED + 7).reshape(-1, 2)
     t0 = time.perf_counter()
-    tot = 0.0
-    for a, b in pairs:
-        _, ms, _ = s.run_state([int(a)], GpuOptions(), astar=True, dst=int(b), copy=False)
-        tot += ms
-    out["astar_32_pairs_mean_ms"] = round(tot / len(pairs), 3)
-    s.close()
+    # --- the 1000x1000 grid: single-source modes and 256 A* pairs ---
+    with pf.GpuSolver(g, 1) as s:
+        src = int(pf.uniform_vertices(g.n, 1, SEED)[0])
+        for algo in (GpuAlgo.DeltaStep, GpuAlgo.Frontier, GpuAlgo.NaiveRelax):
+            o = GpuOptions(algo=algo)
+            out[f"grid1000_sssp_{algo.name}_ms"] = round(_median_ms(lambda: s.run_state([src], o, copy=False)[1], 3), 3)
+        pairs = pf.uniform_vertices(g.n, 2 * 256, SEED + 7).reshape(-1, 2)
+        ts = [s.run_state([int(a)], GpuOptions(), astar=True, dst=int(b), copy=False)[1] for a, b in pairs]
+        out["grid1000_astar_256_pairs_ms"] = {"mean": round(float(np.mean(ts)), 3),
+                                              "p50": round(float(np.percentile(ts, 50)), 3),
+                                              "p99": round(float(np.percentile(ts, 99)), 3)}
+    # --- R-MAT scale 20: learned policy vs fixed automatic Delta (same engine, same sources) ---
+    from pathfinding_gpu_b200 import policy as P
+    if P.WEIGHTS.exists():
+        gr = pf.rmat(20, 16, seed=SEED)
+        with pf.GpuSolver(gr, 1) as s:
+            s.set_policy(P.load())
+            rows = []
+            for src in pf.pick_sources(gr, 3, 99).tolist():
+                fixed = GpuOptions(blockSize=1024)
+                learned = GpuOptions(blockSize=1024, policy=Policy.Learned)
+                tf = _median_ms(lambda: s.run_state([src], fixed, copy=False)[1])
+                tl = _median_ms(lambda: s.run_state([src], learned, copy=False)[1])
+                st_f, _, a = s.run_state([src], fixed)
+                st_l, _, b = s.run_state([src], learned)
+                rows.append({"src": src, "fixed_ms": round(tf, 3), "learned_ms": round(tl, 3),
+                             "speedup": round(tf / tl, 3), "identical_state": bool(np.array_equal(a, b)),
+                             "work_per_m_fixed": round(st_f.edgesScanned / gr.m, 3),
+                             "work_per_m_learned": round(st_l.edgesScanned / gr.m, 3)})
+            out["rmat20_learned_vs_fixed"] = {"median_speedup": statistics.median(r["speedup"] for r in rows),
+                                              "runs": rows}
+    # --- uneven batch in one launch, replayed from a CUDA graph ---
+    from pathfinding_gpu_b200.batch import GpuBatch
+    big = pf.grid(1024, 1024, SEED)
+    small = pf.grid_batch(256, 32, 316, SEED)
+    graphs = [big] + small
+    inst = [(0, int(v)) for v in pf.uniform_vertices(big.n, 64, SEED)]
+    inst += [(i + 1, int(pf.uniform_vertices(gs.n, 1, 100 + i)[0])) for i, gs in enumerate(small)]
+    states = 64 * big.n + sum(gs.n for gs in small)
+    with GpuBatch(graphs, max_states=states, max_instances=len(inst)) as b:
+        b.set_instances(inst)
+        o = GpuOptions(atomic=pf.AtomicMode.MinNoCheck)
+        run_ms = _median_ms(lambda: b.run(o)[1], 3)
+        b.capture(o)
+        rep_ms = _median_ms(lambda: b.replay()[1], 5)
+        arcs = 64 * big.m + sum(gs.m for gs in small)
+        out["batch_uneven"] = {"instances": len(inst), "states": states, "arcs": arcs,
+                               "run_ms": round(run_ms, 3), "replay_ms": round(rep_ms, 3),
+                               "gteps_replay": round(arcs / rep_ms / 1e6, 3)}
+    # --- A* serving with continuous batching on the 2048x2048 road-like graph ---
+    from pathfinding_gpu_b200.serving import GpuServer, run_poisson
+    road = pf.road(2048, seed=SEED)
+    v = pf.uniform_vertices(road.n, 2 * 1000, SEED)
+    qs = [(int(v[2 * i]), int(v[2 * i + 1])) for i in range(1000)]
+    with GpuServer(road, slots=128) as srv:
+        run_poisson(srv, qs[:50], 1000.0, max_rounds=32, seed=2)  # warm
+        rep = run_poisson(srv, qs, 1000.0, max_rounds=32, seed=3, time_limit_s=30)
+        rep.pop("results")
+        out["serving_road2048"] = {k: (round(x, 3) if isinstance(x, float) else x) for k, x in rep.items()}
+    out["extras_wall_s"] = round(time.perf_counter() - t0, 1)
     return out
 
 
