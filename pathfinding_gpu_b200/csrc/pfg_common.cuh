@@ -184,6 +184,7 @@ struct RunParams {
     u32* ring;
     u32 ring_mask;
     u32* aq;           // ring counters, see RingCounter
+    int test_absent_cta;  // test hook: CTA 0 leaves at once, so every barrier wait runs out
 };
 
 // ---------------------------------------------------------------------------

@@ -1115,6 +1115,9 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
     __shared__ float s_feat[POL_IN];
     __shared__ float act0[POL_H], act1[POL_H];
     Local L;
+    // Failure test: with CTA 0 absent no barrier completes; every other CTA's
+    // wait runs into its time limit and the run ends with DS_TIMEOUT.
+    if (p.test_absent_cta && blockIdx.x == 0) return;
 
     if (p.resume) {
         // Continue a paused machine (serving): the round descriptor in the

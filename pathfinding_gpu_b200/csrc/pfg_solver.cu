@@ -498,6 +498,7 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     p.trace = mode == MODE_DELTA ? d_trace : nullptr;
     p.trace_cap = trace_cap;
     p.timeout_ns = device_timeout_ns();
+    p.test_absent_cta = env_int("PFG_TEST_ABSENT_CTA", 0) != 0 ? 1 : 0;
     // Asynchronous buckets for Delta-stepping (see pfg_schedule).
     if (async_buckets_for(o, mode)) {
         p.ring = s->d_ring;

@@ -1,0 +1,35 @@
+"""Failure handling without a GPU fault: every device-side wait is bounded.
+
+With PFG_TEST_ABSENT_CTA=1 the persistent kernel's CTA 0 leaves at once, so no
+grid barrier can complete; every other CTA's wait runs into the PFG_TIMEOUT_MS
+limit, the run ends with PFG_ERR_DEVICE_TIMEOUT (status 5), and the context
+and the solver stay usable: the next run is bit-exact again."""
+import numpy as np
+import pytest
+
+import pathfinding_gpu_b200 as pf
+from pathfinding_gpu_b200 import GpuAlgo, GpuOptions, Schedule
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("opt", [GpuOptions(schedule=Schedule.Rounds), GpuOptions(schedule=Schedule.Async),
+                                 GpuOptions(algo=GpuAlgo.Frontier)])
+def test_barrier_wait_times_out_and_solver_recovers(oracle, monkeypatch, opt):
+    g = pf.grid(40, 40, 3)
+    with pf.GpuSolver(g, 2) as s:
+        monkeypatch.setenv("PFG_TIMEOUT_MS", "100")
+        monkeypatch.setenv("PFG_TEST_ABSENT_CTA", "1")
+        with pytest.raises(RuntimeError) as e:
+            s.sssp(5, opt)
+        assert getattr(e.value, "status", None) == 5, e.value
+        monkeypatch.delenv("PFG_TEST_ABSENT_CTA")
+        r = s.sssp(5, opt)
+        d_ref, p_can = oracle.sssp_canonical(g, 5)
+        assert np.array_equal(r.dist, d_ref) and np.array_equal(r.parent, p_can)
+        stats, ms, state = s.run_state([7, 1500], opt)
+        d, p = pf.unpack(state)
+        for i, src in enumerate((7, 1500)):
+            d_ref, p_can = oracle.sssp_canonical(g, src)
+            assert np.array_equal(d[i * g.n:(i + 1) * g.n], d_ref)
+            assert np.array_equal(p[i * g.n:(i + 1) * g.n], p_can)
