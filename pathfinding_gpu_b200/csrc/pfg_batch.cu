@@ -29,6 +29,7 @@ struct pfg_batch {
     u32 num_graphs = 0;
     std::vector<u32> g_n, g_m, g_rowbase;
     u32 maxw = 0;
+    u32 max_deg = 0;
     double avg_w = 0.0, avg_deg = 0.0;
     u64 max_states = 0;
     u32 max_inst = 0;
@@ -129,6 +130,7 @@ static pfg_status batch_create(pfg_batch* b, uint32_t num_graphs, const uint32_t
         for (u32 u = 0; u < ns[g]; ++u) {
             pr[u] = (u32)pad_total;
             const u32 deg = rows[g][u + 1] - rows[g][u];
+            b->max_deg = std::max(b->max_deg, deg);
             pad_total += (u64)((deg + ROW_ALIGN - 1) / ROW_ALIGN) * ROW_ALIGN;
         }
         pr[ns[g]] = (u32)pad_total;

@@ -54,6 +54,7 @@ struct pfg_solver {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     u32 n = 0, m = 0, K = 1, maxw = 0;
+    u32 max_deg = 0;            // largest out-degree
     u64 m_pad = 0;
     double hscale = 0.0, avg_w = 0.0, avg_deg = 0.0;
     bool has_xy = false;

@@ -156,6 +156,49 @@ __device__ __forceinline__ u32 light_end(const uint2* adj, u32 r0, u32 r1, u32 d
 // claimed list in shared memory, which is relaxed again in the same round
 // (eager sub-rounds) and flushed to the global near queue at the end of the
 // round; only overflow goes to the global queue directly.
+// Appends gv, which this thread has just claimed (near: for the current
+// window; else: for the far pile), to the claimed list, the ring, or a queue.
+__device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, u32 gv, bool near, u32 inst,
+                                             Local& L, Coop* cl) {
+    Ctl* c = p.ctl;
+    L.pushes++;
+    if (!near) {
+        queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gv);
+        if (p.inst_far_cnt) atomicAdd(p.inst_far_cnt + inst, 1u);
+        return;
+    }
+    if (cl) {
+        const u32 slot = atomicAdd(&cl->cl_n, 1u);
+        if (slot - cl->cl_head < CL_CAP) {
+            cl->cl[slot & (CL_CAP - 1u)] = gv;
+            return;
+        }
+    }
+    if (s.async_bkt) {
+        if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, gv, p.timeout_ns))
+            atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+        return;
+    }
+    const u32 out = s.in_buf ^ 1u;
+    queue_push(p.nearq[out], &c->cnt[C_NEAR0 + out], gv);
+}
+
+// After gv's distance was lowered to a value of key `key`: flag it (prefix-scan
+// compaction) or claim it for the window / the far pile and queue it.
+__device__ __forceinline__ void after_improve(const RunParams& p, const Snap& s, u32 gv, u64 key, u32 inst,
+                                              Local& L, Coop* cl) {
+    L.updates++;
+    if (p.prefix_scan) {  // flag only; the COMPACT round builds the next frontier
+        p.near_stamp[gv] = s.near_epoch;
+        L.pushes++;
+        return;
+    }
+    const bool near = key < s.hi;
+    if (!near) L.fmin = key < L.fmin ? key : L.fmin;
+    if (claim_stamp(near ? p.near_stamp : p.far_stamp, gv, near ? s.near_epoch : s.far_epoch))
+        push_claimed(p, s, gv, near, inst, L, cl);
+}
+
 template <bool ASTAR, int AM>
 __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32 u, u32 du,
                                           u32 ib, u64 ub, u32 inst, u32 v, u32 w, Local& L, Coop* cl) {
@@ -170,39 +213,7 @@ __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32
     }
     const u32 gv = ib + v;
     if (!relax_state<AM>(p.state + gv, (u32)nd, u, L.atomics)) return;
-    L.updates++;
-    Ctl* c = p.ctl;
-    if (p.prefix_scan) {  // flag only; the COMPACT round builds the next frontier
-        p.near_stamp[gv] = s.near_epoch;
-        L.pushes++;
-        return;
-    }
-    if (key < s.hi) {
-        if (claim_stamp(p.near_stamp, gv, s.near_epoch)) {
-            L.pushes++;
-            if (cl) {
-                const u32 slot = atomicAdd(&cl->cl_n, 1u);
-                if (slot - cl->cl_head < CL_CAP) {
-                    cl->cl[slot & (CL_CAP - 1u)] = gv;
-                    return;
-                }
-            }
-            if (s.async_bkt) {
-                if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, gv, p.timeout_ns))
-                    atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
-                return;
-            }
-            const u32 out = s.in_buf ^ 1u;
-            queue_push(p.nearq[out], &c->cnt[C_NEAR0 + out], gv);
-        }
-    } else {
-        if (claim_stamp(p.far_stamp, gv, s.far_epoch)) {
-            queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gv);
-            L.pushes++;
-            if (p.inst_far_cnt) atomicAdd(p.inst_far_cnt + inst, 1u);
-        }
-        L.fmin = key < L.fmin ? key : L.fmin;
-    }
+    after_improve(p, s, gv, key, inst, L, cl);
 }
 
 // Thread tier: one thread walks its own arcs [eb, ee) with 128-bit loads
@@ -218,16 +229,9 @@ __device__ __forceinline__ void relax_range_thread(const RunParams& p, const Sna
     }
 }
 
-// Reads one input item (a state index) and decides what to relax: returns
-// false when the item is stale, pruned, or (SCAN) outside the new window -
-// items of a later bucket are carried to the next far pile here. On true,
-// [eb, ee) is the arc range of the round kind (light prefix / heavy suffix).
-template <bool ASTAR>
-__device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32 gi, int kind,
-                                          Local& L, u32& u, u32& ib, u32& du, u64& ub, u32& inst,
-                                          u32& eb, u32& ee) {
-    Ctl* c = p.ctl;
-    u32 rb = 0;  // first padded row start of the item's graph
+// Instance, state base, row base and local vertex of state index gi.
+__device__ __forceinline__ void decode_item(const RunParams& p, u32 gi, u32& inst, u32& ib, u32& rb, u32& u) {
+    rb = 0;  // first padded row start of the item's graph
     if (p.inst_off) {
         // uneven instances: last instance whose offset is <= gi
         u32 lo = 0, hi = p.k - 1;
@@ -243,6 +247,22 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
         ib = inst * p.n;
     }
     u = gi - ib;
+}
+
+// Reads one input item (a state index) and decides what to relax: returns
+// false when the item is stale, pruned, or (SCAN) outside the new window -
+// items of a later bucket are carried to the next far pile here. On true,
+// [eb, ee) is the arc range of the round kind (light prefix / heavy suffix).
+// The row bounds are loaded together with the state word (one round trip),
+// or passed in (pre) by a caller that loaded them earlier.
+template <bool ASTAR>
+__device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32 gi, int kind,
+                                          Local& L, u32& u, u32& ib, u32& du, u64& ub, u32& inst,
+                                          u32& eb, u32& ee, bool pre = false, u32 pr0 = 0u, u32 pr1 = 0u) {
+    Ctl* c = p.ctl;
+    u32 rb;
+    decode_item(p, gi, inst, ib, rb, u);
+    const u32 r0 = pre ? pr0 : __ldg(p.prow + rb + u), r1 = pre ? pr1 : __ldg(p.prow + rb + u + 1);
     du = st_dist(ld_state(p.state + gi));
     bool act = du != INF32;
     u64 key = du;
@@ -267,7 +287,6 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
         }
     }
     if (!act) return false;
-    const u32 r0 = __ldg(p.prow + rb + u), r1 = __ldg(p.prow + rb + u + 1);
     if (kind == K_HEAVY) {
         eb = light_end(p.adj, r0, r1, s.delta);
         ee = r1;
@@ -346,7 +365,7 @@ __device__ __forceinline__ void flush_claimed(const RunParams& p, const Snap& s,
 template <bool ASTAR, int AM, int MAP>
 __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, bool act, u32 u, u32 du,
                                             u32 ib, u64 ub, u32 inst, u32 eb, u32 ee, Local& L, Coop& cs,
-                                            Coop* cl) {
+                                            Coop* cl, int kind) {
     if constexpr (MAP == 0) {  // thread per item
         if (act) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, inst, eb, ee, L);
     } else if constexpr (MAP == 1) {  // warp per item
@@ -389,7 +408,7 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
         bool act = false;
         if (idx < send)
             act = take_item<ASTAR>(p, s, ld_cg(in + idx), kind, L, u, ib, du, ub, inst, eb, ee);
-        relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
+        relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl, kind);
     }
     if constexpr (MAP == 2) {
         if (cl && !s.async_bkt) {  // (asynchronous buckets drain the claimed list themselves)
@@ -415,7 +434,7 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
                         bool act = false;
                         if (idx < hi)
                             act = take_item<ASTAR>(p, s, cs.cl[idx], K_LIGHT, L, u, ib, du, ub, inst, eb, ee);
-                        relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
+                        relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl, K_LIGHT);
                     }
                     lo = hi;
                 }
@@ -573,14 +592,17 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
                 if (gi != RING_EMPTY) *slot = RING_EMPTY;
             }
             if (gi != RING_EMPTY) {
+                u32 i0, b0, rb0, u0;
+                decode_item(p, gi, i0, b0, rb0, u0);
+                const u32 r0 = __ldg(p.prow + rb0 + u0), r1 = __ldg(p.prow + rb0 + u0 + 1);  // in flight across the fence
                 p.near_stamp[gi] = 0u;  // release the claim (epochs start at 1)
                 __threadfence();
-                act = take_item<ASTAR>(p, s, gi, K_LIGHT, L, u, ib, du, ub, inst, eb, ee);
+                act = take_item<ASTAR>(p, s, gi, K_LIGHT, L, u, ib, du, ub, inst, eb, ee, true, r0, r1);
             }
         }
         u32 idle_now = 0u;
         if (threadIdx.x == 0) idle_now = ld_relaxed(aq + AQ_IDLE);
-        relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, MAP == 2 ? &cs : nullptr);
+        relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, MAP == 2 ? &cs : nullptr, K_LIGHT);
         __syncthreads();  // every push of the pass has been performed
         if (threadIdx.x == 0) {
             s_idle = idle_now;

@@ -154,9 +154,11 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
     // Padded row starts: each row rounded up to a multiple of 4 arcs.
     std::vector<u32> prow((size_t)n + 1);
     u64 acc = 0;
+    u32 max_deg = 0;
     for (u32 u = 0; u < n; ++u) {
         prow[u] = (u32)acc;
         const u32 deg = row[u + 1] - row[u];
+        max_deg = std::max(max_deg, deg);
         acc += (u64)((deg + ROW_ALIGN - 1) / ROW_ALIGN) * ROW_ALIGN;
         if (acc >= 0xFFFFFFF0ull) return fail(PFG_ERR_INVALID_GRAPH, "padded arc count exceeds 2^32");
     }
@@ -168,6 +170,7 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
     s->m = m;
     s->K = K;
     s->maxw = maxw;
+    s->max_deg = max_deg;
     s->m_pad = acc;
     s->hscale = h_scale;
     s->avg_w = avg_w;
