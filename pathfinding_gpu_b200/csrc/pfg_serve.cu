@@ -8,7 +8,9 @@
 // different times share one monotone bucket sequence without holding up the
 // ones in flight. The host drives bounded steps: admit waiting queries into
 // free slots, run at most R rounds, collect the slots whose far pile went
-// empty at a bucket advance (their target distance is final), repeat.
+// empty at a bucket advance (their target distance is final), repeat. With
+// asynchronous buckets (the default schedule) a step's budget counts bucket
+// drains: one barrier epoch per bucket.
 // The reference answers one query per GpuSolver::astar call
 // (src/gpu_sssp.cu:549-551); results here are the same distances.
 #include "../../include/pfg.h"
@@ -73,6 +75,8 @@ struct AdmitParams {
     u32* far_cnt;
     u32* active;
     u32* done;
+    u32* aq;     // ring counters (asynchronous buckets), else nullptr
+    u32 grid;    // CTAs of the persistent launch
 };
 
 // Admission and step preparation, one thread: seeds the admitted slots and
@@ -106,6 +110,20 @@ __global__ void k_serve_begin_step(AdmitParams a) {
         c->cnt[C_FAR0] = c->cnt[C_FAR1] = 0u;
         c->cnt[C_R] = 0u;
         c->far_min[0] = c->far_min[1] = ~0ull;
+        r.async_bkt = 0u;
+        if (a.aq) {
+            // asynchronous first bucket: every CTA scans its slice of the seeds
+            // in near queue 0, then drains the ring and its claimed list
+            c->cnt[C_NEAR0] = 0u;
+            r.in_kind = 1u;
+            r.async_bkt = 1u;
+            r.phase = PH_ASYNC;
+            a.aq[AQ_HEAD] = 0u;
+            a.aq[AQ_TAIL] = 0u;
+            a.aq[AQ_DONE] = 0u;
+            a.aq[AQ_BUSY] = a.grid;
+            a.aq[AQ_IDLE] = 0u;
+        }
     }
     for (u32 j = 0; j < a.m; ++j) {
         const u32 s = a.adm_slot[j], src = a.adm_src[j], dst = a.adm_dst[j];
@@ -359,6 +377,9 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
     a.far_cnt = v->d_far_cnt;
     a.active = v->d_active;
     a.done = v->d_done;
+    const bool async = async_buckets_for(v->opt, MODE_DELTA);
+    a.aq = async ? s->d_aq : nullptr;
+    a.grid = (u32)v->grid;
     k_serve_begin_step<<<1, 32, 0, st>>>(a);
     S_CUDA(cudaGetLastError());
 
@@ -405,6 +426,11 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
     if (v->opt.eager < 0 && s->avg_deg > 6.0) p.eager = 0;
     p.eager_max_items = (u32)std::max<long long>(1, (long long)v->grid * v->block / 4);
     p.timeout_ns = device_timeout_ns();
+    if (async) {
+        p.ring = s->d_ring;
+        p.ring_mask = s->ring_mask;
+        p.aq = s->d_aq;
+    }
     cudaError_t le = launch_persistent(p, true, v->opt.atomic, v->opt.mapping, v->block, v->grid, st);
     if (le != cudaSuccess) {
         cudaGetLastError();
@@ -418,7 +444,13 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
     S_CUDA(cudaMemcpyAsync(v->h_rounds, &s->d_ctl->rounds, 4, cudaMemcpyDeviceToHost, st));
     S_CUDA(cudaStreamSynchronize(st));
     v->steps++;
-    if (v->h_rd->status == DS_TIMEOUT) return set_error(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
+    if (v->h_rd->status == DS_TIMEOUT) {
+        // the next step must find the ring empty
+        cudaMemsetAsync(s->d_ring, 0xFF, ((u64)s->ring_mask + 1) * 4, st);
+        cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, st);
+        cudaStreamSynchronize(st);
+        return set_error(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
+    }
     if (v->h_rd->status != DS_OK) return set_error(PFG_ERR_CUDA, "serving machine status %u", v->h_rd->status);
 
     // ---- retire finished slots ----
