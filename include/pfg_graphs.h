@@ -39,6 +39,26 @@ PFG_API pfg_status pfg_graph_from_edges(uint32_t n, uint64_t m_in, const uint32_
                                 const uint32_t* dst, const uint32_t* w, const double* x,
                                 const double* y, pfg_graph** out);
 
+/* The same CSR built on the GPU (self loops dropped, w < 1 raised to 1, rows
+ * sorted by (w, dst), statistics and h_scale): a result identical word for
+ * word to pfg_graph_from_edges, for arc lists too large to sort on the host
+ * quickly (extension; replaces the host counting sort and per-row sort of
+ * buildCSR, src/graph.cpp:23-104). Host arrays in, host graph out. */
+PFG_API pfg_status pfg_graph_from_edges_gpu(uint32_t n, uint64_t m_in, const uint32_t* src,
+                                    const uint32_t* dst, const uint32_t* w, const double* x,
+                                    const double* y, int32_t device, pfg_graph** out);
+
+/* The device part of pfg_graph_from_edges_gpu for arcs already on the GPU:
+ * d_src / d_dst / d_w [m_in], optional d_x / d_y [n]; writes d_row [n+1],
+ * d_col and d_w_out (the first info->m entries, at most m_in) and the
+ * statistics into *info. Allocates its scratch with cudaMalloc; returns after
+ * the work on `stream` (a cudaStream_t, NULL = default stream) is done. */
+PFG_API pfg_status pfg_csr_build_device(uint32_t n, uint64_t m_in, const uint32_t* d_src,
+                                const uint32_t* d_dst, const uint32_t* d_w, const double* d_x,
+                                const double* d_y, uint32_t* d_row, uint32_t* d_col,
+                                uint32_t* d_w_out, pfg_graph_info* info, int32_t device,
+                                void* stream);
+
 /* rows x cols grid at integer coordinates (x = column, y = row), arcs both ways
  * to the 4 neighbours, each arc its own weight llround(100 * U[1.0, 1.5)). */
 PFG_API pfg_status pfg_graph_gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, pfg_graph** out);

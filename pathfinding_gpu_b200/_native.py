@@ -117,6 +117,9 @@ SIGNATURES = {
     "pfg_abi_version": (i32, []),
     # include/pfg_graphs.h
     "pfg_graph_from_edges": (i32, [u32, u64, P(u32), P(u32), P(u32), P(f64), P(f64), P(C.c_void_p)]),
+    "pfg_graph_from_edges_gpu": (i32, [u32, u64, P(u32), P(u32), P(u32), P(f64), P(f64), i32, P(C.c_void_p)]),
+    "pfg_csr_build_device": (i32, [u32, u64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, P(PfgGraphInfo), i32, C.c_void_p]),
     "pfg_graph_gen_grid": (i32, [u32, u32, u64, P(C.c_void_p)]),
     "pfg_graph_gen_rmat": (i32, [u32, u32, f64, f64, f64, u32, u32, u64, P(C.c_void_p)]),
     "pfg_graph_gen_road": (i32, [u32, f64, f64, u32, f64, u64, P(C.c_void_p)]),

@@ -23,7 +23,7 @@ NVCC_FLAGS = ARCH + [
     "-I", str(ROOT / "include"),
 ]
 SOURCES = ["pfg_kernels.cu", "pfg_solver.cu", "pfg_device.cu", "pfg_policy.cu", "pfg_batch.cu",
-           "pfg_serve.cu", "pfg_noalloc.cu", "pfg_graphs.cpp"]
+           "pfg_serve.cu", "pfg_noalloc.cu", "pfg_csr.cu", "pfg_graphs.cpp"]
 HEADERS = ["pfg_common.cuh", "pfg_kernels.h", "pfg_internal.h"]
 
 

@@ -156,6 +156,28 @@ pfg_status build_csr(u32 n, const std::vector<u32>& src, const std::vector<u32>&
     return PFG_OK;
 }
 
+}  // namespace
+
+// Wraps CSR arrays that are already in final form (built on the GPU by
+// pfg_graph_from_edges_gpu) into a graph handle.
+pfg_status pfg_internal_graph_from_csr(uint32_t n, std::vector<uint32_t>&& row, std::vector<uint32_t>&& col,
+                                       std::vector<uint32_t>&& w, std::vector<double>&& x,
+                                       std::vector<double>&& y, const pfg_graph_info& info, pfg_graph** out) {
+    pfg_graph* g = new pfg_graph();
+    g->n = n;
+    g->m = info.m;
+    g->row = std::move(row);
+    g->col = std::move(col);
+    g->w = std::move(w);
+    g->x = std::move(x);
+    g->y = std::move(y);
+    g->info = info;
+    *out = g;
+    return PFG_OK;
+}
+
+namespace {
+
 inline u32 grid_weight(SplitMix& rng) { return (u32)std::llround(100.0 * rng.uniform(1.0, 1.5)); }
 
 }  // namespace

@@ -112,8 +112,11 @@ def _gen(fn_name: str, *args, name: str = "") -> CSRGraph:
     return CSRGraph._from_handle(h, name)
 
 
-def buildCSR(n: int, src, dst, w, x=None, y=None, name: str = "") -> CSRGraph:
-    """CSR from an arc list (reference buildCSR, src/graph.cpp:23-104)."""
+def buildCSR(n: int, src, dst, w, x=None, y=None, name: str = "", device: Optional[int] = None) -> CSRGraph:
+    """CSR from an arc list (reference buildCSR, src/graph.cpp:23-104).
+
+    device=None builds on the host; device=d sorts and counts on GPU d
+    (pfg_graph_from_edges_gpu), with an identical result."""
     src = np.ascontiguousarray(src, np.uint32)
     dst = np.ascontiguousarray(dst, np.uint32)
     w = np.ascontiguousarray(w, np.uint32)
@@ -121,6 +124,9 @@ def buildCSR(n: int, src, dst, w, x=None, y=None, name: str = "") -> CSRGraph:
     y = None if y is None else np.ascontiguousarray(y, np.float64)
     if not (len(src) == len(dst) == len(w)):
         raise ValueError("src, dst and w must have the same length")
+    if device is not None:
+        return _gen("pfg_graph_from_edges_gpu", n, len(src), N.ptr(src, N.u32), N.ptr(dst, N.u32),
+                    N.ptr(w, N.u32), N.ptr(x, N.f64), N.ptr(y, N.f64), int(device), name=name)
     return _gen("pfg_graph_from_edges", n, len(src), N.ptr(src, N.u32), N.ptr(dst, N.u32),
                 N.ptr(w, N.u32), N.ptr(x, N.f64), N.ptr(y, N.f64), name=name)
 
