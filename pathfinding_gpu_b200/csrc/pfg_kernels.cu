@@ -360,6 +360,53 @@ __device__ __forceinline__ void flush_claimed(const RunParams& p, const Snap& s,
 // ---------------------------------------------------------------------------
 // One round over an input array of items (state indices).
 // ---------------------------------------------------------------------------
+// Position of this thread's item in a chunk of blockDim.x items: item i goes to
+// lane i / W of warp i % W (W warps), so a partly filled chunk spreads over all
+// warps instead of filling the first ones.
+__device__ __forceinline__ u32 item_slot() {
+    const u32 W = blockDim.x >> 5;
+    return (threadIdx.x & 31u) * W + (threadIdx.x >> 5);
+}
+
+// Warp-balanced relaxation: each warp numbers the selected arcs of its own
+// lanes' items with a shuffle scan and deals them out one per lane (owner found
+// by a 5-step shuffle search), with no block barrier. Used when no item of the
+// CTA has more than WARP_ROW_MAX selected arcs, so a warp never carries a hub.
+constexpr u32 WARP_ROW_MAX = 32;
+template <bool ASTAR, int AM>
+__device__ __forceinline__ void relax_items_warp(const RunParams& p, const Snap& s, bool act, u32 u, u32 du,
+                                                 u32 ib, u64 ub, u32 inst, u32 eb, u32 ee, Local& L, Coop* cl) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 sz = act ? ee - eb : 0u;
+    u32 x = sz;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(FULL, x, o);
+        if (lane >= (u32)o) x += y;
+    }
+    const u32 total = __shfl_sync(FULL, x, 31);
+    const u32 off = x - sz;
+    for (u32 j0 = 0; j0 < total; j0 += 32) {  // warp-uniform
+        const u32 j = j0 + lane;
+        // owner = last lane whose offset is <= j (empty items repeat offsets)
+        u32 lo = 0;
+#pragma unroll
+        for (u32 step = 16; step > 0; step >>= 1) {
+            const u32 cand = lo + step;
+            if (__shfl_sync(FULL, off, cand) <= j) lo = cand;
+        }
+        const u32 wu = __shfl_sync(FULL, u, lo), wdu = __shfl_sync(FULL, du, lo);
+        const u32 wib = __shfl_sync(FULL, ib, lo), winst = __shfl_sync(FULL, inst, lo);
+        const u32 web = __shfl_sync(FULL, eb, lo), woff = __shfl_sync(FULL, off, lo);
+        u64 wub = ~0ull;
+        if constexpr (ASTAR) wub = __shfl_sync(FULL, ub, lo);
+        if (j < total) {
+            const uint2 a = __ldg(p.adj + web + (j - woff));
+            relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, winst, a.x, a.y, L, cl);
+        }
+    }
+}
+
 // Relaxes the selected arcs of the items held by the CTA's threads (at most one
 // item per thread) with the mapping MAP. Called by every thread of the CTA.
 template <bool ASTAR, int AM, int MAP>
@@ -384,7 +431,11 @@ __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, b
             }
         }
     } else {
-        relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
+        // short rows only: each warp balances its own items; else the CTA does
+        if (__syncthreads_or(act && ee - eb > WARP_ROW_MAX))
+            relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
+        else
+            relax_items_warp<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cl);
     }
 }
 
@@ -402,7 +453,7 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
     const u32 sbeg = min(count, blockIdx.x * per);
     const u32 send = min(count, sbeg + per);
     for (u32 base = sbeg; base < send; base += BS) {
-        const u32 idx = base + threadIdx.x;
+        const u32 idx = base + item_slot();
         u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, inst = 0;
         u64 ub = ~0ull;
         bool act = false;
@@ -428,7 +479,7 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
                     __syncthreads();
                     if (hi <= lo) break;  // block-uniform
                     for (u32 base = lo; base < hi; base += BS) {
-                        const u32 idx = base + threadIdx.x;
+                        const u32 idx = base + item_slot();
                         u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, inst = 0;
                         u64 ub = ~0ull;
                         bool act = false;
@@ -571,12 +622,13 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
         u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, inst = 0;
         u64 ub = ~0ull;
         bool act = false;
-        if (threadIdx.x < n) {
+        const u32 my = item_slot();
+        if (my < n) {
             u32 gi;
             if (src == 1u) {
-                gi = cs.cl[(h + threadIdx.x) & CLM];
+                gi = cs.cl[(h + my) & CLM];
             } else {
-                u32* slot = p.ring + ((h + threadIdx.x) & p.ring_mask);
+                u32* slot = p.ring + ((h + my) & p.ring_mask);
                 gi = ld_relaxed(slot);
                 if (gi == RING_EMPTY) {
                     // reserved by a producer that has not written it yet
@@ -692,40 +744,41 @@ __device__ void round_compact(const RunParams& p, const Snap& s, Coop& cs) {
 }
 
 // ---------------------------------------------------------------------------
-// Learned Delta policy: 12 features -> 3 x 64 ReLU -> 8 logits; the argmax
-// picks a multiple of the automatic Delta. Evaluated by the CTA that runs a
-// bucket-advance transition.
+// Learned Delta policy: 12 features -> 3 x 64 ReLU -> 16 logits; the argmax
+// picks the next bucket's schedule and multiple of the automatic Delta.
+// Evaluated by the CTA that runs a bucket-advance transition.
 // ---------------------------------------------------------------------------
+// One dense layer out[j] = act(b[j] + sum_i w[j * NI + i] * in[i]) by the
+// whole CTA: G threads per neuron (a power of two dividing 32) each sum a
+// strided share of the inputs, then a shuffle reduction within the group.
+template <int NI, int NO, bool RELU>
+__device__ __forceinline__ void policy_layer(const float* __restrict__ w, const float* __restrict__ b,
+                                             const float* in, float* out) {
+    const u32 t = threadIdx.x, BS = blockDim.x;
+    const u32 G = BS >= 256u ? 4u : 1u;
+    const u32 part = t & (G - 1u);
+    for (u32 j = t / G; j < (u32)NO; j += BS / G) {  // uniform within each warp (NO * G % 32 == 0)
+        float a = 0.f;
+        for (u32 i = part; i < (u32)NI; i += G) a = fmaf(__ldg(w + j * NI + i), in[i], a);
+        for (u32 o = G >> 1; o > 0; o >>= 1) a += __shfl_down_sync(FULL, a, o, G);
+        if (part == 0) {
+            a += __ldg(b + j);
+            out[j] = RELU ? (a > 0.f ? a : 0.f) : a;
+        }
+    }
+    __syncthreads();
+}
+
 __device__ u32 policy_pick(const PolicyNet* net, const float* feat, float* act0, float* act1) {
     const u32 t = threadIdx.x;
     __shared__ float s_in[POL_IN];
     __shared__ float s_logit[POL_OUT];
     if (t < POL_IN) s_in[t] = (feat[t] - net->in_mean[t]) * net->in_scale[t];
     __syncthreads();
-    if (t < POL_H) {
-        float a = net->b1[t];
-        for (int i = 0; i < POL_IN; ++i) a = fmaf(net->w1[t * POL_IN + i], s_in[i], a);
-        act0[t] = a > 0.f ? a : 0.f;
-    }
-    __syncthreads();
-    if (t < POL_H) {
-        float a = net->b2[t];
-        for (int i = 0; i < POL_H; ++i) a = fmaf(net->w2[t * POL_H + i], act0[i], a);
-        act1[t] = a > 0.f ? a : 0.f;
-    }
-    __syncthreads();
-    if (t < POL_H) {
-        float a = net->b3[t];
-        for (int i = 0; i < POL_H; ++i) a = fmaf(net->w3[t * POL_H + i], act1[i], a);
-        act0[t] = a > 0.f ? a : 0.f;
-    }
-    __syncthreads();
-    if (t < POL_OUT) {
-        float a = net->b4[t];
-        for (int i = 0; i < POL_H; ++i) a = fmaf(net->w4[t * POL_H + i], act0[i], a);
-        s_logit[t] = a;
-    }
-    __syncthreads();
+    policy_layer<POL_IN, POL_H, true>(net->w1, net->b1, s_in, act0);
+    policy_layer<POL_H, POL_H, true>(net->w2, net->b2, act0, act1);
+    policy_layer<POL_H, POL_H, true>(net->w3, net->b3, act1, act0);
+    policy_layer<POL_H, POL_OUT, false>(net->w4, net->b4, act0, s_logit);
     u32 best = 0;
     for (u32 i = 1; i < (u32)POL_OUT; ++i)
         if (s_logit[i] > s_logit[best]) best = i;

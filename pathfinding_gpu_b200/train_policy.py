@@ -2,7 +2,7 @@
 
     python -m pathfinding_gpu_b200.train_policy [--out policy_weights.npz] [--report report.json]
 
-1. Traces: for every (graph, source) of the training families (R-MAT scales 18-20
+1. Traces: for every (graph, source) of the training families (R-MAT scales 19-20
    with two edge factors and two weight ranges, seeds other than the evaluation
    graph's; grids of 256-768 per side; a road-like grid), fixed-Delta
    runs of each class of policy.CLASSES (schedule x multiplier) are timed and
@@ -28,11 +28,12 @@ from . import policy as P
 from .solver import GpuOptions, GpuSolver, Policy, unpack
 
 TRAIN_FAMILIES = [
-    ("rmat_s18_ef16_w255", lambda: G.rmat(18, 16, w_lo=1, w_hi=255, seed=15)),
     ("rmat_s19_ef16_w255", lambda: G.rmat(19, 16, w_lo=1, w_hi=255, seed=16)),
     ("rmat_s19_ef8_w1000", lambda: G.rmat(19, 8, w_lo=1, w_hi=1000, seed=17)),
     ("rmat_s20_ef8_w255", lambda: G.rmat(20, 8, w_lo=1, w_hi=255, seed=18)),
     ("rmat_s20_ef16_w255_seed31", lambda: G.rmat(20, 16, w_lo=1, w_hi=255, seed=31)),
+    ("rmat_s20_ef16_w255_seed32", lambda: G.rmat(20, 16, w_lo=1, w_hi=255, seed=32)),
+    ("rmat_s20_ef16_w255_seed33", lambda: G.rmat(20, 16, w_lo=1, w_hi=255, seed=33)),
     ("grid_256", lambda: G.grid(256, 256, 21)),
     ("grid_512", lambda: G.grid(512, 512, 22)),
     ("grid_768", lambda: G.grid(768, 768, 23)),
@@ -53,7 +54,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(P.WEIGHTS))
     ap.add_argument("--report", default=None)
-    ap.add_argument("--sources", type=int, default=3)
+    ap.add_argument("--sources", type=int, default=4)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--lr", type=float, default=3e-3)
     args = ap.parse_args(argv)
