@@ -30,6 +30,7 @@ struct pfg_batch {
     std::vector<u32> g_n, g_m, g_rowbase;
     u32 maxw = 0;
     u32 max_deg = 0;
+    u64 hub_rows = 0;  // vertices with more than 256 arcs (all graphs)
     double avg_w = 0.0, avg_deg = 0.0;
     u64 max_states = 0;
     u32 max_inst = 0;
@@ -50,6 +51,8 @@ struct pfg_batch {
     u32* d_ring = nullptr;  // ring queue of asynchronous buckets, RING_EMPTY when idle
     u32 ring_mask = 0;
     u32* d_aq = nullptr;    // ring counters
+    HubRec* d_hubs = nullptr;  // hub records of the grid tier
+    u32 hub_cap = 0;
     Ctl* d_ctl = nullptr;
     Ctl* h_ctl_init = nullptr;  // pinned: the control block every run starts from
     Ctl* h_ctl_out = nullptr;   // pinned: the control block every run ends with
@@ -131,6 +134,7 @@ static pfg_status batch_create(pfg_batch* b, uint32_t num_graphs, const uint32_t
             pr[u] = (u32)pad_total;
             const u32 deg = rows[g][u + 1] - rows[g][u];
             b->max_deg = std::max(b->max_deg, deg);
+            b->hub_rows += deg > 256u ? 1u : 0u;
             pad_total += (u64)((deg + ROW_ALIGN - 1) / ROW_ALIGN) * ROW_ALIGN;
         }
         pr[ns[g]] = (u32)pad_total;
@@ -201,6 +205,13 @@ static pfg_status batch_create(pfg_batch* b, uint32_t num_graphs, const uint32_t
     if (st == PFG_OK) st = b->dalloc(&b->d_aq, (u64)AQ_WORDS);
     if (st != PFG_OK) return st;
     b->ring_mask = (u32)(ring - 1);
+    if (b->hub_rows) {
+        // instances may repeat a graph: bound by the states, a hub row has > 256 arcs
+        b->hub_cap = (u32)std::min<u64>(std::max<u64>(1024, 2 * b->hub_rows * std::max<u64>(1, b->max_inst)), 1u << 24);
+        st = b->dalloc(&b->d_hubs, (u64)b->hub_cap);
+        if (st != PFG_OK) return st;
+        B_CUDA(cudaMemsetAsync(b->d_hubs, 0, (size_t)b->hub_cap * sizeof(HubRec), b->stream));
+    }
     B_CUDA(cudaMemsetAsync(b->d_ring, 0xFF, ring * 4, b->stream));
     B_CUDA(cudaMemsetAsync(b->d_aq, 0, AQ_WORDS * 4, b->stream));
     for (int i = 0; i < 3; ++i) B_CUDA(cudaMemsetAsync(b->d_stamp[i], 0, S * 4, b->stream));
@@ -335,6 +346,13 @@ static pfg_status batch_prepare(pfg_batch* b, const pfg_options* opt_in, RunPara
         p.aq = b->d_aq;
     }
     block = o.block_size;
+    if (b->d_hubs && o.mapping == PFG_MAP_HYBRID && b->max_deg > 8u * (u32)block) {
+        p.hubs = b->d_hubs;
+        p.hub_cap = b->hub_cap;
+        p.hub_min = 8u * (u32)block;
+        p.hub_chunk = 4u * (u32)block;
+        p.aq = b->d_aq;
+    }
     const int bps = blocks_per_sm_for(o, false, o.mapping);
     if (bps <= 0) return set_error(PFG_ERR_CUDA, "occupancy query failed for block size %d", block);
     grid = b->sm_count * bps;

@@ -47,8 +47,22 @@ enum Phase : u32 {
 
 // Ring queue of the asynchronous bucket phase: counters in RunParams::aq, one
 // 128-byte line each (u32 index).
-enum RingCounter : u32 { AQ_HEAD = 0, AQ_TAIL = 32, AQ_DONE = 64, AQ_BUSY = 96, AQ_IDLE = 128, AQ_WORDS = 160 };
+enum RingCounter : u32 { AQ_HEAD = 0, AQ_TAIL = 32, AQ_DONE = 64, AQ_BUSY = 96, AQ_IDLE = 128, AQ_HUBS = 160,
+                         AQ_WORDS = 192 };
 constexpr u32 RING_EMPTY = 0xFFFFFFFFu;  // a free ring slot
+
+// Grid tier of the hybrid mapping: an item whose selected arcs exceed
+// RunParams::hub_min is published as a hub record, and any CTA claims chunks
+// of hub_chunk arcs of it (aq[AQ_HUBS] counts the records of the current
+// round / bucket drain; records are valid for the round descriptor's near
+// epoch only, so nothing is cleared between rounds).
+struct __align__(32) HubRec {
+    u32 gi, eb, ee;  // state index of the item, its selected arc range
+    u32 ready;       // near epoch of the round that published it (fields visible)
+    u32 next;        // next unclaimed arc offset (atomicAdd by hub_chunk)
+    u32 done;        // arcs relaxed (asynchronous buckets: the last chunk ends the record's busy unit)
+    u32 pad0, pad1;
+};
 
 // Run modes (reference GpuAlgo, include/gpu_sssp.h:10-14).
 enum RunMode : int { MODE_NAIVE = 0, MODE_FRONTIER = 1, MODE_DELTA = 2 };
@@ -185,6 +199,10 @@ struct RunParams {
     u32 ring_mask;
     u32* aq;           // ring counters, see RingCounter
     int test_absent_cta;  // test hook: CTA 0 leaves at once, so every barrier wait runs out
+    HubRec* hubs;      // hub records (nullptr: no row of the graph is long enough)
+    u32 hub_cap;       // records available
+    u32 hub_min;       // items with more selected arcs are published as hubs
+    u32 hub_chunk;     // arcs per claimed chunk
 };
 
 // ---------------------------------------------------------------------------

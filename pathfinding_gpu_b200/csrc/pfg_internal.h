@@ -55,6 +55,7 @@ struct pfg_solver {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     u32 n = 0, m = 0, K = 1, maxw = 0;
     u32 max_deg = 0;            // largest out-degree
+    u64 hub_rows = 0;           // vertices with more than 256 arcs
     u64 m_pad = 0;
     double hscale = 0.0, avg_w = 0.0, avg_deg = 0.0;
     bool has_xy = false;
@@ -74,6 +75,8 @@ struct pfg_solver {
     u32* d_ring = nullptr;      // ring queue of asynchronous buckets [ring_mask + 1], RING_EMPTY when idle
     u32 ring_mask = 0;
     u32* d_aq = nullptr;        // ring counters [AQ_WORDS]
+    pfg::HubRec* d_hubs = nullptr;  // hub records of the grid tier [hub_cap]
+    u32 hub_cap = 0;
     u32* d_srcs = nullptr;
     u32* d_path = nullptr;      // path extraction scratch [n + 1]
     u32* d_path_len = nullptr;

@@ -439,6 +439,78 @@ __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, b
     }
 }
 
+// Publishes the hub row [eb, ee) of item gi; false if the record table is
+// full (the caller then relaxes the row itself). In an asynchronous drain
+// (phase ASYNC) the record holds a busy unit until its last chunk is relaxed;
+// in a round every CTA works the round's records before the barrier.
+__device__ __forceinline__ bool hub_publish(const RunParams& p, const Snap& s, u32 gi, u32 eb, u32 ee) {
+    const bool drain = s.phase == PH_ASYNC;
+    if (drain) atomicAdd(p.aq + AQ_BUSY, 1u);
+    const u32 k = atomicAdd(p.aq + AQ_HUBS, 1u);
+    if (k >= p.hub_cap) {
+        if (drain) atomicSub(p.aq + AQ_BUSY, 1u);
+        return false;
+    }
+    HubRec* r = p.hubs + k;
+    r->gi = gi;
+    r->eb = eb;
+    r->ee = ee;
+    r->next = 0u;
+    r->done = 0u;
+    __threadfence();
+    atomicExch(&r->ready, s.near_epoch);
+    return true;
+}
+
+// Claims the next chunk of a published hub row (records from the CTA's cursor
+// s_hub[0] on; records without a chunk left are passed for good) and relaxes it
+// with the whole CTA. Returns false if no chunk could be claimed. On true,
+// s_hub[1] is the record and [s_hub[3], s_hub[4]) the chunk. Called by every
+// thread of the CTA.
+template <bool ASTAR, int AM>
+__device__ bool hub_chunk(const RunParams& p, const Snap& s, Local& L, Coop* cl, u32* s_hub) {
+    __shared__ u32 s_u, s_du, s_ib, s_inst;
+    __shared__ u64 s_ub;
+    if (threadIdx.x == 0) {
+        u32 k = s_hub[0], found = 0;
+        const u32 cnt = min(ld_relaxed(p.aq + AQ_HUBS), p.hub_cap);
+        for (; k < cnt; ++k) {
+            HubRec* r = p.hubs + k;
+            if (ld_acquire(&r->ready) != s.near_epoch) continue;  // not (yet) published: its owner relaxes it
+            const u32 eb = __ldcg(&r->eb), ee = __ldcg(&r->ee);
+            const u32 off = atomicAdd(&r->next, p.hub_chunk);
+            if (off < ee - eb) {
+                found = 1u;
+                const u32 gi = __ldcg(&r->gi);
+                s_hub[1] = k;
+                s_hub[3] = eb + off;
+                s_hub[4] = min(ee, eb + off + p.hub_chunk);
+                u32 inst, ib, rb, u;
+                decode_item(p, gi, inst, ib, rb, u);
+                s_u = u;
+                s_ib = ib;
+                s_inst = inst;
+                s_du = st_dist(ld_state(p.state + gi));
+                s_ub = ~0ull;
+                if constexpr (ASTAR) s_ub = astar_bound(p, inst, ib);
+                break;
+            }
+        }
+        s_hub[0] = k;
+        s_hub[5] = found;
+    }
+    __syncthreads();
+    if (!s_hub[5]) return false;  // block-uniform
+    const u32 u = s_u, du = s_du, ib = s_ib, inst = s_inst;
+    const u64 ub = s_ub;
+    for (u32 e = s_hub[3] + threadIdx.x; e < s_hub[4]; e += blockDim.x) {
+        const uint2 a = __ldg(p.adj + e);
+        relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, inst, a.x, a.y, L, cl);
+    }
+    __syncthreads();  // every push of the chunk has been performed
+    return true;
+}
+
 template <bool ASTAR, int AM, int MAP>
 __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u32 count, int kind,
                             Local& L, Coop& cs) {
@@ -457,9 +529,26 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
         u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, inst = 0;
         u64 ub = ~0ull;
         bool act = false;
-        if (idx < send)
-            act = take_item<ASTAR>(p, s, ld_cg(in + idx), kind, L, u, ib, du, ub, inst, eb, ee);
+        u32 gi = 0;
+        if (idx < send) {
+            gi = ld_cg(in + idx);
+            act = take_item<ASTAR>(p, s, gi, kind, L, u, ib, du, ub, inst, eb, ee);
+        }
+        if constexpr (MAP == 2) {  // hub rows go to the grid tier
+            if (act && p.hubs && ee - eb > p.hub_min && hub_publish(p, s, gi, eb, ee)) act = false;
+        }
         relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl, kind);
+    }
+    if constexpr (MAP == 2) {
+        if (p.hubs && s.phase != PH_ASYNC) {
+            // rounds: chunks of every hub record of the round before the barrier
+            // (a CTA that published a record relaxes what nobody else claimed)
+            __shared__ u32 s_hub[8];
+            if (threadIdx.x == 0) s_hub[0] = 0u;
+            __syncthreads();
+            while (hub_chunk<ASTAR, AM>(p, s, L, cl, s_hub)) {
+            }
+        }
     }
     if constexpr (MAP == 2) {
         if (cl && !s.async_bkt) {  // (asynchronous buckets drain the claimed list themselves)
@@ -518,6 +607,7 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
 template <bool ASTAR, int AM, int MAP>
 __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& cs, bool busy_held) {
     __shared__ u32 s_src, s_h, s_n, s_spill, s_spill_from, s_spill_base, s_busy, s_idle;
+    __shared__ u32 s_hub[8];
     constexpr u32 CLM = CL_CAP - 1u;
     const u32 G = gridDim.x, BS = blockDim.x;
     u32* aq = p.aq;
@@ -525,6 +615,7 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
     if (threadIdx.x == 0) {
         s_busy = busy_held ? 1u : 0u;
         s_idle = 0u;
+        s_hub[0] = 0u;
     }
     for (;;) {
         __syncthreads();
@@ -535,7 +626,10 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
             cs.cl_n = tail;
             const u32 local = tail - cs.cl_head;
             u32 src = 0, h = 0, n = 0, spill = 0;
-            if (local > 0u) {
+            if (p.hubs && min(ld_relaxed(aq + AQ_HUBS), p.hub_cap) > s_hub[0]) {
+                src = 3u;  // chunks of hub rows first: they are the longest chains
+                n = 1u;
+            } else if (local > 0u) {
                 src = 1u;
                 h = cs.cl_head;
                 n = local < BS ? local : BS;
@@ -577,6 +671,11 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
                         }
                         continue;  // another CTA took these positions first
                     }
+                    if (p.hubs && min(ld_relaxed(aq + AQ_HUBS), p.hub_cap) > s_hub[0]) {
+                        src = 3u;
+                        n = 1u;
+                        break;
+                    }
                     if (busy == 0u && done == t) break;  // the bucket is drained
                     if (!idle) {
                         atomicAdd(aq + AQ_IDLE, 1u);
@@ -598,6 +697,19 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
         __syncthreads();
         const u32 src = s_src, h = s_h, n = s_n, spill = s_spill;
         if (n == 0u) break;  // block-uniform
+        if (src == 3u) {
+            if (hub_chunk<ASTAR, AM>(p, s, L, MAP == 2 ? &cs : nullptr, s_hub) && threadIdx.x == 0) {
+                if (cs.cl_n != cs.cl_head && !s_busy) {
+                    atomicAdd(aq + AQ_BUSY, 1u);
+                    s_busy = 1u;
+                    __threadfence();  // busy is raised before the record can end
+                }
+                HubRec* r = p.hubs + s_hub[1];
+                const u32 d = s_hub[4] - s_hub[3];
+                if (atomicAdd(&r->done, d) + d == __ldcg(&r->ee) - __ldcg(&r->eb)) atomicSub(aq + AQ_BUSY, 1u);
+            }
+            continue;
+        }
         if (spill) {
             // the newest part of the backlog goes to the ring for idle CTAs
             const u32 from = s_spill_from, base = s_spill_base;
@@ -650,6 +762,7 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
                 p.near_stamp[gi] = 0u;  // release the claim (epochs start at 1)
                 __threadfence();
                 act = take_item<ASTAR>(p, s, gi, K_LIGHT, L, u, ib, du, ub, inst, eb, ee, true, r0, r1);
+                if (MAP == 2 && act && p.hubs && ee - eb > p.hub_min && hub_publish(p, s, gi, eb, ee)) act = false;
             }
         }
         u32 idle_now = 0u;
@@ -855,6 +968,7 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
     if (t == 0) {
         Rd& r = sc.rd;
         s_flag[0] = 0;
+        if (p.hubs) p.aq[AQ_HUBS] = 0u;  // hub records live for one round / bucket drain
         const u32 ph = r.phase;
         const u32 rounds = sc.rounds;
         const u32 in_buf = r.in_buf;

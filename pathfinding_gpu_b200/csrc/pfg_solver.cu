@@ -155,10 +155,12 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
     std::vector<u32> prow((size_t)n + 1);
     u64 acc = 0;
     u32 max_deg = 0;
+    u64 hub_rows = 0;  // rows long enough to be hubs for the smallest CTA (8 x 32 arcs)
     for (u32 u = 0; u < n; ++u) {
         prow[u] = (u32)acc;
         const u32 deg = row[u + 1] - row[u];
         max_deg = std::max(max_deg, deg);
+        hub_rows += deg > 256u ? 1u : 0u;
         acc += (u64)((deg + ROW_ALIGN - 1) / ROW_ALIGN) * ROW_ALIGN;
         if (acc >= 0xFFFFFFF0ull) return fail(PFG_ERR_INVALID_GRAPH, "padded arc count exceeds 2^32");
     }
@@ -171,6 +173,7 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
     s->K = K;
     s->maxw = maxw;
     s->max_deg = max_deg;
+    s->hub_rows = hub_rows;
     s->m_pad = acc;
     s->hscale = h_scale;
     s->avg_w = avg_w;
@@ -297,6 +300,13 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
     s->ring_mask = (u32)(ring - 1);
     TRY(s->dalloc(&s->d_aq, (u64)AQ_WORDS));
     TRYC(cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, s->stream));
+    // Hub records: every instance's hub rows once per round, twice over for
+    // re-published rows of an asynchronous drain (overflow falls back to the CTA).
+    if (s->hub_rows) {
+        s->hub_cap = (u32)std::min<u64>(std::max<u64>(1024, 2 * (u64)K * s->hub_rows), 1u << 24);
+        TRY(s->dalloc(&s->d_hubs, (u64)s->hub_cap));
+        TRYC(cudaMemsetAsync(s->d_hubs, 0, (size_t)s->hub_cap * sizeof(HubRec), s->stream));
+    }
     TRY(s->dalloc(&s->d_srcs, K));
     TRY(s->dalloc(&s->d_path, (u64)n + 1));
     TRY(s->dalloc(&s->d_path_len, 1));
@@ -511,6 +521,14 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
 
     const int map = mode == MODE_NAIVE ? PFG_MAP_THREAD : o.mapping;
     const int block = o.block_size;
+    // Grid tier of the hybrid mapping for rows longer than 8 CTAs' worth of arcs.
+    if (s->d_hubs && map == PFG_MAP_HYBRID && mode != MODE_NAIVE && s->max_deg > 8u * (u32)block) {
+        p.hubs = s->d_hubs;
+        p.hub_cap = s->hub_cap;
+        p.hub_min = 8u * (u32)block;
+        p.hub_chunk = 4u * (u32)block;
+        p.aq = s->d_aq;
+    }
     const int bps = blocks_per_sm_for(o, astar != 0, map);
     if (bps <= 0) return fail(PFG_ERR_CUDA, "occupancy query failed for block size %d", block);
     const int grid = s->sm_count * bps;

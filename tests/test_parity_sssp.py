@@ -192,3 +192,66 @@ def test_errors_like_reference(grid100_solver):
         grid100_solver.multiSource(list(range(18)), GpuOptions(), None)
     # the solver stays usable after an error
     assert grid100_solver.sssp(0, GpuOptions()).dist[0] == 0
+
+
+@pytest.fixture(scope="module")
+def hub_graph():
+    # random arcs plus three long rows (25,000 / 9,000 / 3,000 arcs), so rows
+    # exceed 8 x the block size and take the grid tier of the hybrid mapping
+    rng = np.random.default_rng(7)
+    n = 30000
+    src = [rng.integers(0, n, 200000)]
+    dst = [rng.integers(0, n, 200000)]
+    for h, L in ((0, 25000), (17, 9000), (12345, 3000)):
+        src.append(np.full(L, h))
+        dst.append(rng.integers(0, n, L))
+    src = np.concatenate(src).astype(np.uint32)
+    dst = np.concatenate(dst).astype(np.uint32)
+    w = rng.integers(1, 200, len(src)).astype(np.uint32)
+    x = rng.uniform(0, 1000, n)
+    y = rng.uniform(0, 1000, n)
+    return pf.buildCSR(n, src, dst, w, x, y)
+
+
+@pytest.mark.parametrize("schedule", SCHEDULES)
+@pytest.mark.parametrize("block,atomic", [(32, AtomicMode.MinRBA), (64, AtomicMode.MinNoCheck),
+                                          (256, AtomicMode.MinRBA), (256, AtomicMode.CasRBA),
+                                          (1024, AtomicMode.MinNoCheck)])
+def test_hub_rows_grid_tier(oracle, hub_graph, schedule, block, atomic):
+    g = hub_graph
+    with pf.GpuSolver(g, 4) as s:
+        for src in (0, 17, 5):
+            for delta in (0, 20):
+                res = s.sssp(src, GpuOptions(blockSize=block, atomic=atomic, schedule=schedule, delta=delta))
+                check_sssp(oracle, g, src, res)
+        srcs = [0, 17, 12345, 9]
+        _, _, state = s.run_state(srcs, GpuOptions(blockSize=block, atomic=atomic, schedule=schedule))
+        dist, parent = pf.unpack(state)
+        for i, src in enumerate(srcs):
+            d_ref, p_can = oracle.sssp_canonical(g, src)
+            assert np.array_equal(dist[i * g.n:(i + 1) * g.n], d_ref), (schedule, block, i)
+            assert np.array_equal(parent[i * g.n:(i + 1) * g.n], p_can), (schedule, block, i)
+
+
+def test_hub_rows_astar_and_batch(oracle, hub_graph):
+    from pathfinding_gpu_b200.batch import GpuBatch
+    g = hub_graph
+    with pf.GpuSolver(g, 1) as s:
+        for src, dst in ((0, 29999), (17, 4), (12345, 100)):
+            d_ref = oracle.dijkstra(g, src)[0]
+            for schedule in SCHEDULES:
+                r = s.astar(src, dst, GpuOptions(blockSize=64, schedule=schedule))
+                assert r.targetDist == d_ref[dst]
+                if d_ref[dst] != 0xFFFFFFFF:
+                    assert oracle.validate_path(g, r.path, src, dst, int(d_ref[dst]))
+    small = pf.grid(20, 20, 3)
+    with GpuBatch([g, small], max_instances=4, max_states=3 * g.n + small.n) as b:
+        inst = [(0, 0), (1, 5), (0, 17), (0, 12345)]
+        b.set_instances(inst)
+        for schedule in SCHEDULES:
+            b.run(GpuOptions(blockSize=128, schedule=schedule))
+            state = b.state()
+            for i, (gi, src) in enumerate(inst):
+                d, p = b.instance_result(i, state)
+                d_ref, p_can = oracle.sssp_canonical([g, small][gi], src)
+                assert np.array_equal(d, d_ref) and np.array_equal(p, p_can), (schedule, i)
