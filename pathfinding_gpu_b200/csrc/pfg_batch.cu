@@ -169,17 +169,20 @@ static pfg_status batch_create(pfg_batch* b, uint32_t num_graphs, const uint32_t
     pfg_status st = b->dalloc(&b->d_adj, pad_total);
     if (st == PFG_OK) st = b->dalloc(&b->d_prow, rows_total);
     if (st != PFG_OK) return st;
+    // Every copy is ordered on the batch's stream, before the kernel that reads
+    // it: the stream does not synchronise with the legacy default stream, and a
+    // pageable cudaMemcpy may return before its DMA has landed.
     for (u32 g = 0; g < num_graphs; ++g) {
         const u32 n = ns[g], m = ms[g];
         u32 *d_row = nullptr, *d_col = nullptr, *d_w = nullptr;
-        B_CUDA(cudaMemcpy(b->d_prow + b->g_rowbase[g], prows[g].data(), ((size_t)n + 1) * 4,
-                          cudaMemcpyHostToDevice));
+        B_CUDA(cudaMemcpyAsync(b->d_prow + b->g_rowbase[g], prows[g].data(), ((size_t)n + 1) * 4,
+                               cudaMemcpyHostToDevice, b->stream));
         B_CUDA(cudaMalloc((void**)&d_row, ((size_t)n + 1) * 4));
         cudaError_t e = cudaMalloc((void**)&d_col, std::max<size_t>(1, (size_t)m) * 4);
         if (e == cudaSuccess) e = cudaMalloc((void**)&d_w, std::max<size_t>(1, (size_t)m) * 4);
-        if (e == cudaSuccess) e = cudaMemcpy(d_row, rows[g], ((size_t)n + 1) * 4, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess && m) e = cudaMemcpy(d_col, cols[g], (size_t)m * 4, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess && m) e = cudaMemcpy(d_w, ws[g], (size_t)m * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_row, rows[g], ((size_t)n + 1) * 4, cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess && m) e = cudaMemcpyAsync(d_col, cols[g], (size_t)m * 4, cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess && m) e = cudaMemcpyAsync(d_w, ws[g], (size_t)m * 4, cudaMemcpyHostToDevice, b->stream);
         if (e == cudaSuccess) e = launch_build_adj(d_row, d_col, d_w, b->d_prow + b->g_rowbase[g], n, b->d_adj, b->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
         cudaFree(d_row);
@@ -271,9 +274,11 @@ extern "C" pfg_status pfg_batch_set_instances(pfg_batch* b, const uint32_t* inst
     off[count] = (u32)acc;
     B_CUDA(cudaSetDevice(b->device));
     B_CUDA(cudaStreamSynchronize(b->stream));
-    B_CUDA(cudaMemcpy(b->d_inst_off, off.data(), ((size_t)count + 1) * 4, cudaMemcpyHostToDevice));
-    B_CUDA(cudaMemcpy(b->d_inst_rowbase, rb.data(), (size_t)count * 4, cudaMemcpyHostToDevice));
-    B_CUDA(cudaMemcpy(b->d_srcs, inst_src, (size_t)count * 4, cudaMemcpyHostToDevice));
+    // ordered on the batch's stream, which does not wait for the legacy stream
+    B_CUDA(cudaMemcpyAsync(b->d_inst_off, off.data(), ((size_t)count + 1) * 4, cudaMemcpyHostToDevice, b->stream));
+    B_CUDA(cudaMemcpyAsync(b->d_inst_rowbase, rb.data(), (size_t)count * 4, cudaMemcpyHostToDevice, b->stream));
+    B_CUDA(cudaMemcpyAsync(b->d_srcs, inst_src, (size_t)count * 4, cudaMemcpyHostToDevice, b->stream));
+    B_CUDA(cudaStreamSynchronize(b->stream));
     b->inst_off = off;
     b->num_inst = count;
     b->total_states = acc;
@@ -297,7 +302,8 @@ static pfg_status batch_prepare(pfg_batch* b, const pfg_options* opt_in, RunPara
         Ctl c0;
         memset(&c0, 0, sizeof(c0));
         c0.near_epoch = c0.far_epoch = c0.r_epoch = 1;
-        B_CUDA(cudaMemcpy(b->d_ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice));
+        B_CUDA(cudaMemcpyAsync(b->d_ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
+        B_CUDA(cudaStreamSynchronize(b->stream));
         b->epoch_hint = 1;
     }
     Ctl* c = b->h_ctl_init;
@@ -403,7 +409,8 @@ static pfg_status batch_complete(pfg_batch* b, int mode, u32 delta, pfg_stats* s
             cudaMemsetAsync(b->d_ring, 0xFF, ((u64)b->ring_mask + 1) * 4, b->stream);
             cudaMemsetAsync(b->d_aq, 0, AQ_WORDS * 4, b->stream);
             cudaStreamSynchronize(b->stream);
-            return set_error(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
+            return set_error(PFG_ERR_DEVICE_TIMEOUT, "device-side wait timed out: %s made no progress for %llu ms",
+                             wait_site_name(c->wait_site), (unsigned long long)(device_timeout_ns() / 1000000ull));
         default: return set_error(PFG_ERR_CUDA, "device status %u", c->rd.status);
     }
 }

@@ -48,7 +48,11 @@ enum Phase : u32 {
 // Ring queue of the asynchronous bucket phase: counters in RunParams::aq, one
 // 128-byte line each (u32 index).
 enum RingCounter : u32 { AQ_HEAD = 0, AQ_TAIL = 32, AQ_DONE = 64, AQ_BUSY = 96, AQ_IDLE = 128, AQ_HUBS = 160,
-                         AQ_WORDS = 192 };
+                         AQ_BEAT = 192, AQ_WORDS = 224 };
+// AQ_BEAT: heartbeat, bumped by every working pass of an asynchronous drain. A
+// CTA that waits (for work, or at the barrier after leaving a drain) measures its
+// time limit from the last change of the heartbeat, so a long but progressing
+// drain (one CTA walking a long chain) never reads as a hang.
 constexpr u32 RING_EMPTY = 0xFFFFFFFFu;  // a free ring slot
 
 // Grid tier of the hybrid mapping: an item whose selected arcs exceed
@@ -73,6 +77,21 @@ enum CounterSlot : u32 { C_NEAR0 = 0, C_NEAR1 = 1, C_FAR0 = 2, C_FAR1 = 3, C_R =
 // Device status words (match pfg_status values).
 enum DevStatus : u32 { DS_OK = 0, DS_BAD_SOURCE = 1, DS_NOT_CONVERGED = 4, DS_TIMEOUT = 5 };
 
+// Which device-side wait ran out of time (Ctl::wait_site; outside the words a
+// transition stores back, so a concurrent transition never erases it).
+enum WaitSite : u32 { WS_NONE = 0, WS_RING_PUSH = 1, WS_DRAIN_IDLE = 2, WS_SPILL_SLOT = 3, WS_RING_SLOT = 4,
+                      WS_BARRIER = 5 };
+inline const char* wait_site_name(u32 w) {
+    switch (w) {
+        case WS_RING_PUSH: return "a ring-queue push waiting for a free slot";
+        case WS_DRAIN_IDLE: return "an idle CTA of an asynchronous bucket waiting for work";
+        case WS_SPILL_SLOT: return "a claimed-list spill waiting for a free ring slot";
+        case WS_RING_SLOT: return "a ring-queue pop waiting for its item to be written";
+        case WS_BARRIER: return "the grid barrier";
+    }
+    return "a device-side wait";
+}
+
 // Round descriptor: everything a CTA needs to run the next round. Written by
 // the transition, read by every CTA with five 16-byte loads after a barrier.
 struct __align__(16) Rd {
@@ -93,7 +112,8 @@ struct __align__(16) Rd {
 struct __align__(16) Ctl {
     u32 bar_count;     // barrier tickets taken in this run (grows by gridDim.x per barrier)
     u32 bar_gen;       // barriers completed in this run
-    u32 pad_b0, pad_b1;
+    u32 wait_site;     // WaitSite of the first wait that ran out of time (0: none)
+    u32 pad_b1;
     Rd rd;
     u32 rounds;        // barrier epochs so far
     u32 iterations;    // rounds with a non-empty input
@@ -229,6 +249,13 @@ __device__ __forceinline__ u32 ld_acquire(const u32* p) {
     return v;
 }
 __device__ __forceinline__ u64 vload64(const u64* p) { return *(const volatile u64*)p; }
+
+// Records that the wait at `site` ran out of time (the first such wait names
+// the site) and ends the run with DS_TIMEOUT.
+__device__ __forceinline__ void flag_timeout(Ctl* c, u32 site) {
+    atomicCAS(&c->wait_site, (u32)WS_NONE, site);
+    atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+}
 
 __device__ __forceinline__ u32 st_dist(u64 s) { return (u32)(s >> 32); }
 __device__ __forceinline__ u64 pack_state(u32 d, u32 p) { return ((u64)d << 32) | (u64)p; }

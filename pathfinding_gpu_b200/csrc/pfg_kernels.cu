@@ -175,8 +175,7 @@ __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, 
         }
     }
     if (s.async_bkt) {
-        if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, gv, p.timeout_ns))
-            atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+        if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, gv, p.timeout_ns)) flag_timeout(c, WS_RING_PUSH);
         return;
     }
     const u32 out = s.in_buf ^ 1u;
@@ -644,12 +643,18 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
                     s_busy = 0u;
                 }
                 bool idle = false;
-                const u64 t0 = global_timer_ns();
+                u64 t0 = global_timer_ns();
+                u32 beat = ld_relaxed(aq + AQ_BEAT);
                 for (u32 spin = 1;; ++spin) {
                     if ((spin & 15u) == 0u) {
                         if (vload(&c->rd.status) != DS_OK) break;
-                        if (global_timer_ns() - t0 > p.timeout_ns) {
-                            atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                        const u64 now = global_timer_ns();
+                        const u32 b = ld_relaxed(aq + AQ_BEAT);
+                        if (b != beat) {  // another CTA made progress: the wait is not a hang
+                            beat = b;
+                            t0 = now;
+                        } else if (now - t0 > p.timeout_ns) {
+                            flag_timeout(c, WS_DRAIN_IDLE);
                             break;
                         }
                     }
@@ -697,6 +702,7 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
         __syncthreads();
         const u32 src = s_src, h = s_h, n = s_n, spill = s_spill;
         if (n == 0u) break;  // block-uniform
+        if (threadIdx.x == 0) atomicAdd(aq + AQ_BEAT, 1u);
         if (src == 3u) {
             if (hub_chunk<ASTAR, AM>(p, s, L, MAP == 2 ? &cs : nullptr, s_hub) && threadIdx.x == 0) {
                 if (cs.cl_n != cs.cl_head && !s_busy) {
@@ -720,7 +726,7 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
                     const u64 t0 = global_timer_ns();
                     while (atomicCAS(slot, RING_EMPTY, gi) != RING_EMPTY) {
                         if (global_timer_ns() - t0 > p.timeout_ns) {
-                            atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                            flag_timeout(c, WS_SPILL_SLOT);
                             break;
                         }
                         __nanosleep(64);
@@ -747,7 +753,7 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
                     const u64 t0 = global_timer_ns();
                     while ((gi = ld_relaxed(slot)) == RING_EMPTY) {
                         if (global_timer_ns() - t0 > p.timeout_ns) {
-                            atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                            flag_timeout(c, WS_RING_SLOT);
                             break;
                         }
                         __nanosleep(32);
@@ -1265,14 +1271,20 @@ __device__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, Ct
             s = sc.rd;
         }
     } else if (threadIdx.x == 0) {
-        const u64 t0 = global_timer_ns();
+        u64 t0 = global_timer_ns();
+        u32 beat = p.aq ? ld_relaxed(p.aq + AQ_BEAT) : 0u;
         u32 spins = 0;
         bool ok = true;
         while (vload(&c->bar_gen) <= s_gen) {
             if ((++spins & 255u) == 0u) {
                 if (vload(&c->rd.status) != DS_OK) break;
-                if (global_timer_ns() - t0 > p.timeout_ns) {
-                    atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_TIMEOUT);
+                const u64 now = global_timer_ns();
+                const u32 b = p.aq ? ld_relaxed(p.aq + AQ_BEAT) : 0u;
+                if (b != beat) {  // a CTA still draining its bucket made progress
+                    beat = b;
+                    t0 = now;
+                } else if (now - t0 > p.timeout_ns) {
+                    flag_timeout(c, WS_BARRIER);
                     ok = false;
                     break;
                 }

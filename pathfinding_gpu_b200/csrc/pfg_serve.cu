@@ -252,13 +252,15 @@ static pfg_status server_setup(pfg_server* v) {
     S_CUDA(cudaMalloc((void**)&v->d_done, S * 4));
     S_CUDA(cudaMalloc((void**)&v->d_adm, 3 * S * 4));
     S_CUDA(cudaMalloc((void**)&v->d_out, S * 8));
-    S_CUDA(cudaMemset(v->d_target, 0, S * 4));
-    S_CUDA(cudaMemset(v->d_far_cnt, 0, S * 4));
-    S_CUDA(cudaMemset(v->d_active, 0, S * 4));
-    S_CUDA(cudaMemset(v->d_done, 0, S * 4));
-    S_CUDA(cudaMemset(v->d_phi, 0, S * 8));
-    S_CUDA(cudaMemset(v->d_tx, 0, S * 8));
-    S_CUDA(cudaMemset(v->d_ty, 0, S * 8));
+    // cleared on the solver's stream, which does not wait for the legacy stream
+    cudaStream_t st0 = v->s->stream;
+    S_CUDA(cudaMemsetAsync(v->d_target, 0, S * 4, st0));
+    S_CUDA(cudaMemsetAsync(v->d_far_cnt, 0, S * 4, st0));
+    S_CUDA(cudaMemsetAsync(v->d_active, 0, S * 4, st0));
+    S_CUDA(cudaMemsetAsync(v->d_done, 0, S * 4, st0));
+    S_CUDA(cudaMemsetAsync(v->d_phi, 0, S * 8, st0));
+    S_CUDA(cudaMemsetAsync(v->d_tx, 0, S * 8, st0));
+    S_CUDA(cudaMemsetAsync(v->d_ty, 0, S * 8, st0));
     S_CUDA(cudaMallocHost((void**)&v->h_adm, 3 * S * 4));
     S_CUDA(cudaMallocHost((void**)&v->h_out, S * 8));
     S_CUDA(cudaMallocHost((void**)&v->h_done, S * 4));
@@ -442,6 +444,7 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
     S_CUDA(cudaMemcpyAsync(v->h_done, v->d_done, S * 4, cudaMemcpyDeviceToHost, st));
     S_CUDA(cudaMemcpyAsync(v->h_rd, &s->d_ctl->rd, sizeof(Rd), cudaMemcpyDeviceToHost, st));
     S_CUDA(cudaMemcpyAsync(v->h_rounds, &s->d_ctl->rounds, 4, cudaMemcpyDeviceToHost, st));
+    S_CUDA(cudaMemcpyAsync(v->h_rounds + 1, &s->d_ctl->wait_site, 4, cudaMemcpyDeviceToHost, st));
     S_CUDA(cudaStreamSynchronize(st));
     v->steps++;
     if (v->h_rd->status == DS_TIMEOUT) {
@@ -449,7 +452,8 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
         cudaMemsetAsync(s->d_ring, 0xFF, ((u64)s->ring_mask + 1) * 4, st);
         cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, st);
         cudaStreamSynchronize(st);
-        return set_error(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
+        return set_error(PFG_ERR_DEVICE_TIMEOUT, "device-side wait timed out: %s made no progress for %llu ms",
+                         wait_site_name(v->h_rounds[1]), (unsigned long long)(device_timeout_ns() / 1000000ull));
     }
     if (v->h_rd->status != DS_OK) return set_error(PFG_ERR_CUDA, "serving machine status %u", v->h_rd->status);
 

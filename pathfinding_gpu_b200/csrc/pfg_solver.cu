@@ -272,8 +272,10 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
     if (s->has_xy) {
         TRY(s->dalloc(&s->d_x, n));
         TRY(s->dalloc(&s->d_y, n));
-        TRYC(cudaMemcpy(s->d_x, x, (size_t)n * 8, cudaMemcpyHostToDevice));
-        TRYC(cudaMemcpy(s->d_y, y, (size_t)n * 8, cudaMemcpyHostToDevice));
+        // on the solver's stream: it does not wait for the legacy default stream
+        TRYC(cudaMemcpyAsync(s->d_x, x, (size_t)n * 8, cudaMemcpyHostToDevice, s->stream));
+        TRYC(cudaMemcpyAsync(s->d_y, y, (size_t)n * 8, cudaMemcpyHostToDevice, s->stream));
+        TRYC(cudaStreamSynchronize(s->stream));
         s->hx.assign(x, x + n);
         s->hy.assign(y, y + n);
     }
@@ -585,7 +587,8 @@ static pfg_status complete_run(pfg_solver* s, pfg_stats* stats_out) {
         cudaMemsetAsync(s->d_ring, 0xFF, ((u64)s->ring_mask + 1) * 4, s->stream);
         cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, s->stream);
         cudaStreamSynchronize(s->stream);
-        return fail(PFG_ERR_DEVICE_TIMEOUT, "a device-side barrier wait timed out");
+        return fail(PFG_ERR_DEVICE_TIMEOUT, "device-side wait timed out: %s made no progress for %llu ms",
+                    wait_site_name(c->wait_site), (unsigned long long)(device_timeout_ns() / 1000000ull));
     }
     if (status == DS_NOT_CONVERGED) {
         const u64 words = (u64)s->n / 32 + 1;
@@ -717,7 +720,12 @@ extern "C" pfg_status pfg_set_policy(pfg_solver* s, const float* params, uint64_
         return fail(PFG_ERR_INVALID_ARGUMENT, "policy image has %llu floats, expected %llu",
                     (unsigned long long)count, (unsigned long long)(sizeof(PolicyNet) / sizeof(float)));
     PFG_CUDA(cudaSetDevice(s->device));
-    PFG_CUDA(cudaMemcpy(s->d_net, params, sizeof(PolicyNet), cudaMemcpyHostToDevice));
+    if (s->pending) {
+        pfg_status st = complete_run(s, nullptr);
+        if (st != PFG_OK) return st;
+    }
+    PFG_CUDA(cudaMemcpyAsync(s->d_net, params, sizeof(PolicyNet), cudaMemcpyHostToDevice, s->stream));
+    PFG_CUDA(cudaStreamSynchronize(s->stream));
     s->has_net = true;
     return PFG_OK;
 }

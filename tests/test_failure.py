@@ -33,3 +33,18 @@ def test_barrier_wait_times_out_and_solver_recovers(oracle, monkeypatch, opt):
             d_ref, p_can = oracle.sssp_canonical(g, src)
             assert np.array_equal(d[i * g.n:(i + 1) * g.n], d_ref)
             assert np.array_equal(p[i * g.n:(i + 1) * g.n], p_can)
+
+
+def test_long_progressing_drain_is_not_a_timeout(oracle, monkeypatch):
+    # A 100,000-vertex path with one huge bucket: one CTA walks the chain for
+    # far longer than the 100 ms wait limit while every other CTA waits. The
+    # limit counts from the last progress anywhere, so the run succeeds.
+    n = 100000
+    src = np.arange(n - 1, dtype=np.uint32)
+    g = pf.buildCSR(n, src, src + 1, np.full(n - 1, 3, np.uint32))
+    monkeypatch.setenv("PFG_TIMEOUT_MS", "100")
+    with pf.GpuSolver(g, 1) as s:
+        r = s.sssp(0, GpuOptions(schedule=Schedule.Async, delta=1 << 30))
+    assert r.dist[-1] == 3 * (n - 1) and r.parent[-1] == n - 2
+    d_ref, p_can = oracle.sssp_canonical(g, 0)
+    assert np.array_equal(r.dist, d_ref) and np.array_equal(r.parent, p_can)
