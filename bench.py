@@ -10,9 +10,10 @@ over the batch).
 
   value  device time of the step with the graph, sources and working set resident
          in HBM (CUDA events on the solver's stream, L2 flushed between steps)
-  e2e    the same step through the C ABI pfg_run with host buffers: H2D of the K
-         sources from pinned memory, the run, and D2H of the K*n packed state
-         words into pinned memory, timed on the device
+  e2e    the same step through the C ABI as the reference's multiSource with distOut
+         (pfg_run + pfg_copy_dist): H2D of the K sources from pinned memory, the run,
+         the distances of the K*n states split from the packed words on the device and
+         copied into pinned memory, timed on the device
   --impl reference   the reference's own cpuMultiSource (OpenMP, every host thread)
          on the same graph and sources, compiled from its sources into oracle/_ref
   extras (N = 1, skipped with --no-extras): single-source Delta / Frontier / Naive and
@@ -237,7 +238,7 @@ def run_ours(args, D):
     traffic = ncu_traffic("k_persistent_grid1000_k64")
 
     # ---- end to end through the C ABI with host buffers ----
-    h_state = torch.empty(K * g.n, dtype=torch.int64).pin_memory()
+    h_dist = torch.empty(K * g.n, dtype=torch.int32).pin_memory()
     h_srcs = np.ascontiguousarray(srcs, np.uint32)
     st = N.PfgStats()
     ms_c = C.c_float()
@@ -246,7 +247,9 @@ def run_ours(args, D):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         N.check(lib.pfg_run(solver.handle, N.ptr(h_srcs, N.u32), K, 0, 0, C.byref(copt), C.byref(st),
-                            C.cast(C.c_void_p(h_state.data_ptr()), C.POINTER(C.c_uint64)), C.byref(ms_c)))
+                            None, C.byref(ms_c)))
+        N.check(lib.pfg_copy_dist(solver.handle, 0, K * g.n,
+                                  C.cast(C.c_void_p(h_dist.data_ptr()), C.POINTER(C.c_uint32))))
         b.record(stream)
         if i >= args.warmup:
             e2e_evs.append((a, b))
@@ -254,7 +257,7 @@ def run_ours(args, D):
     e2e_ms = D.max(sum(a.elapsed_time(b) for a, b in e2e_evs) / len(e2e_evs))
     e2e_value = arcs_all / (e2e_ms * 1e-3) / 1e9
     # the copied-back result must be the device result
-    got = (h_state.numpy().view(np.uint64) >> np.uint64(32)).astype(np.uint32).reshape(K, g.n)
+    got = h_dist.numpy().view(np.uint32).reshape(K, g.n)
     assert np.array_equal(got, dist), "e2e result differs from the device-resident run"
 
     result = {
@@ -275,8 +278,9 @@ def run_ours(args, D):
                      "bytes_alg_per_launch": bytes_alg,
                      "bytes_model": "16 B per reachable arc + 20 B per reachable vertex, per instance"},
         "e2e": {"value": round(e2e_value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 4 * K + 256,
-                "d2h_bytes_per_step": 8 * K * g.n + 256, "ms_per_step": round(e2e_ms, 4),
-                "api": "pfg_run (C ABI) with pinned host buffers"},
+                "d2h_bytes_per_step": 4 * K * g.n + 256, "ms_per_step": round(e2e_ms, 4),
+                "api": "pfg_run + pfg_copy_dist (C ABI; the reference's multiSource with distOut) "
+                       "with pinned host buffers"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "stats": {"rounds": stats0.rounds, "buckets": stats0.buckets,

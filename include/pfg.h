@@ -171,6 +171,13 @@ PFG_API const uint64_t* pfg_state_device(const pfg_solver* s);
 /* Copies state words [first, first+count) of the last run to host memory. */
 PFG_API pfg_status pfg_copy_state(pfg_solver* s, uint64_t first, uint64_t count, uint64_t* h_out);
 
+/* Copies the distances of state words [first, first+count) of the last run to
+ * host memory, h_out[i] = dist of word first+i: the result of the reference's
+ * GpuSolver::multiSource with distOut (src/gpu_sssp.cu:553-569, which copies
+ * the packed words and splits them on the host). The split runs on the device,
+ * so half the bytes cross PCIe. */
+PFG_API pfg_status pfg_copy_dist(pfg_solver* s, uint64_t first, uint64_t count, uint32_t* h_out);
+
 /* Reconstructs the path src -> dst of instance `inst` of the last run on the
  * device by following parent pointers (reference: reconstructPath,
  * src/cpu_sssp.cpp:124-135). path_len_out = 0 when dst is unreachable or the

@@ -86,6 +86,7 @@ SIGNATURES = {
     "pfg_finish": (i32, [C.c_void_p, P(PfgStats)]),
     "pfg_state_device": (C.c_void_p, [C.c_void_p]),
     "pfg_copy_state": (i32, [C.c_void_p, u64, u64, P(u64)]),
+    "pfg_copy_dist": (i32, [C.c_void_p, u64, u64, P(u32)]),
     "pfg_extract_path": (i32, [C.c_void_p, u32, u32, u32, P(u32), u32, P(u32)]),
     "pfg_query_device": (i32, [i32, P(PfgDeviceInfo)]),
     "pfg_warmup": (i32, []),

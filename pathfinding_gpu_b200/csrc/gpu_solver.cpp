@@ -189,16 +189,16 @@ GpuRunResult GpuSolver::astar(u32 src, u32 dst, const GpuOptions& opt) {
 GpuRunResult GpuSolver::multiSource(const std::vector<u32>& srcs, const GpuOptions& opt,
                                     std::vector<std::vector<u32>>* distOut) {
     const u32 k = (u32)srcs.size();
-    GpuRunResult r = p_->run(srcs.data(), k, false, 0, opt, distOut != nullptr);
+    // k == 1 fills r.dist / r.parent as well, as the reference does; for k > 1
+    // only the distances come back, split from the packed words on the device.
+    GpuRunResult r = p_->run(srcs.data(), k, false, 0, opt, distOut != nullptr && k == 1);
     if (distOut) {
         const u32 n = p_->g.n;
         distOut->assign(k, std::vector<u32>(n));
         if (k == 1) {
             (*distOut)[0] = r.dist;
         } else {
-            for (u32 i = 0; i < k; ++i)
-                for (u32 v = 0; v < n; ++v) (*distOut)[i][v] = (u32)(p_->state[(size_t)i * n + v] >> 32);
-            std::vector<u64>().swap(p_->state);
+            for (u32 i = 0; i < k; ++i) check(pfg_copy_dist(p_->h, (uint64_t)i * n, n, (*distOut)[i].data()));
         }
     }
     return r;

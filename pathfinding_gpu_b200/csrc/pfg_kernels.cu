@@ -1501,4 +1501,24 @@ cudaError_t launch_extract_path(const uint64_t* state, uint64_t base, uint32_t n
     return cudaGetLastError();
 }
 
+// Distance halves of packed state words, out[i] = state[i] >> 32: the
+// reference's per-source distance extraction (src/gpu_sssp.cu:561-565) done
+// on the device, so a multi-source result crosses PCIe at 4 bytes per state.
+// Bandwidth-bound: 8 bytes read and 4 written per word, 16 words per thread
+// in flight per grid-stride pass.
+__global__ void k_extract_dist(const u64* __restrict__ state, u64 count, u32* __restrict__ out) {
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+        out[i] = (u32)(__ldcs(state + i) >> 32);
+}
+
+cudaError_t launch_extract_dist(const uint64_t* state, uint64_t count, uint32_t* out, int sm_count,
+                                cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    const u64 want = (count + 255) / 256;
+    const u64 cap = (u64)(sm_count > 0 ? sm_count : 148) * 16;
+    k_extract_dist<<<(unsigned)(want < cap ? want : cap), 256, 0, st>>>(state, count, out);
+    return cudaGetLastError();
+}
+
 }  // namespace pfg

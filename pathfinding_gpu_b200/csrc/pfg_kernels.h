@@ -26,4 +26,8 @@ cudaError_t launch_extract_path(const uint64_t* state, uint64_t base, uint32_t n
                                 uint32_t src, uint32_t dst, uint32_t* path_rev, uint32_t cap,
                                 uint32_t* len, cudaStream_t st);
 
+// out[i] = distance half of state[i] for i < count (grid of at most 16 CTAs per SM).
+cudaError_t launch_extract_dist(const uint64_t* state, uint64_t count, uint32_t* out, int sm_count,
+                                cudaStream_t st);
+
 }  // namespace pfg

@@ -683,6 +683,23 @@ extern "C" pfg_status pfg_copy_state(pfg_solver* s, uint64_t first, uint64_t cou
     return PFG_OK;
 }
 
+extern "C" pfg_status pfg_copy_dist(pfg_solver* s, uint64_t first, uint64_t count, uint32_t* h_out) {
+    if (!s || (count > 0 && !h_out)) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (first + count > (u64)s->K * s->n) return fail(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
+    PFG_CUDA(cudaSetDevice(s->device));
+    if (s->pending) {
+        pfg_status st = complete_run(s, nullptr);
+        if (st != PFG_OK) return st;
+    }
+    if (count == 0) return PFG_OK;
+    // near queue 0 (K*n words) is free scratch between runs
+    cudaError_t e = launch_extract_dist(s->d_state + first, count, s->d_q[0], s->sm_count, s->stream);
+    if (e != cudaSuccess) return fail(PFG_ERR_CUDA, "distance extraction: %s", cudaGetErrorString(e));
+    PFG_CUDA(cudaMemcpyAsync(h_out, s->d_q[0], count * 4, cudaMemcpyDeviceToHost, s->stream));
+    PFG_CUDA(cudaStreamSynchronize(s->stream));
+    return PFG_OK;
+}
+
 extern "C" pfg_status pfg_extract_path(pfg_solver* s, uint32_t inst, uint32_t src, uint32_t dst,
                                        uint32_t* h_path, uint32_t cap, uint32_t* path_len_out) {
     if (!s || !path_len_out || (cap > 0 && !h_path)) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");

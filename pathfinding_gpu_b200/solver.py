@@ -243,13 +243,22 @@ class GpuSolver:
                     distOut: Optional[list] = None) -> GpuRunResult:
         srcs = np.ascontiguousarray(srcs, np.uint32)
         k = len(srcs)
-        stats, ms, state = self.run_state(srcs, opt, copy=distOut is not None)
+        stats, ms, _ = self.run_state(srcs, opt, copy=False)
         r = GpuRunResult(ms=ms, stats=stats)
         if distOut is not None:
-            dist, _ = unpack(state)
+            dist = self.copy_dist(0, k * self.n)
             distOut.clear()
             distOut.extend(dist.reshape(k, self.n))
         return r
+
+    def copy_dist(self, first: int, count: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Distances of state words [first, first+count) of the last run (split from
+        the packed words on the device; 4 bytes per word cross PCIe)."""
+        if out is None:
+            out = np.empty(count, np.uint32)
+        assert out.dtype == np.uint32 and out.flags.c_contiguous and out.size >= count
+        N.check(self._lib.pfg_copy_dist(self.handle, int(first), int(count), N.ptr(out, N.u32)))
+        return out[:count]
 
     def set_policy(self, params: np.ndarray) -> None:
         params = np.ascontiguousarray(params, np.float32)

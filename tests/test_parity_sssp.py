@@ -13,6 +13,7 @@ import pytest
 
 import pathfinding_gpu_b200 as pf
 from pathfinding_gpu_b200 import GpuAlgo, GpuOptions, Mapping, AtomicMode, Compaction, Schedule
+from pathfinding_gpu_b200 import _native as N
 
 pytestmark = pytest.mark.gpu
 
@@ -163,6 +164,25 @@ def test_grid100_multisource(oracle, grid100, grid100_solver, schedule):
             d_ref, p_can = oracle.sssp_canonical(grid100, s)
             assert np.array_equal(dist[i], d_ref), (algo, i)
             assert np.array_equal(parent[i], p_can), (algo, i)
+
+
+def test_multisource_dist_out_split_on_device(oracle, grid100, grid100_solver):
+    # multiSource with distOut copies only the distance halves (split on the
+    # device); any sub-range, odd starts included, matches the packed words
+    srcs = sources_c0(grid100)
+    dist_out = []
+    grid100_solver.multiSource(srcs, GpuOptions(), dist_out)
+    assert len(dist_out) == len(srcs)
+    for i, s in enumerate(srcs):
+        assert np.array_equal(dist_out[i], oracle.sssp_canonical(grid100, s)[0]), i
+    state = np.empty(len(srcs) * grid100.n, np.uint64)
+    N.check(grid100_solver._lib.pfg_copy_state(grid100_solver.handle, 0, state.size, N.ptr(state, N.u64)))
+    for first, count in ((0, state.size), (1, 3), (grid100.n - 1, 2 * grid100.n + 5), (state.size - 1, 1),
+                         (7, 0)):
+        got = grid100_solver.copy_dist(first, count)
+        assert np.array_equal(got, (state[first:first + count] >> np.uint64(32)).astype(np.uint32))
+    with pytest.raises(pf.PfgError):
+        grid100_solver.copy_dist(state.size - 1, 2)
 
 
 def test_rmat_variants(oracle, rmat12, rmat12_solver):
