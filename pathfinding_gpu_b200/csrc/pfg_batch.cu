@@ -48,7 +48,7 @@ struct pfg_batch {
     u32* d_inst_off = nullptr;
     u32* d_inst_rowbase = nullptr;
     u32* d_srcs = nullptr;
-    u32* d_ring = nullptr;  // ring queue of asynchronous buckets, RING_EMPTY when idle
+    unsigned long long* d_ring = nullptr;  // ring queue of asynchronous buckets, RING_FREE when idle
     u32 ring_mask = 0;
     u32* d_aq = nullptr;    // ring counters
     HubRec* d_hubs = nullptr;  // hub records of the grid tier
@@ -202,8 +202,8 @@ static pfg_status batch_create(pfg_batch* b, uint32_t num_graphs, const uint32_t
     if (st == PFG_OK) st = b->dalloc(&b->d_inst_rowbase, b->max_inst);
     if (st == PFG_OK) st = b->dalloc(&b->d_srcs, b->max_inst);
     if (st == PFG_OK) st = b->dalloc(&b->d_ctl, 1);
-    u64 ring = 1024;
-    while (ring < S) ring <<= 1;
+    u64 ring = 1024;  // room for two entries per state (one per strict improvement in flight)
+    while (ring < 2 * (u64)S && ring < (1ull << 32)) ring <<= 1;
     if (st == PFG_OK) st = b->dalloc(&b->d_ring, ring);
     if (st == PFG_OK) st = b->dalloc(&b->d_aq, (u64)AQ_WORDS);
     if (st != PFG_OK) return st;
@@ -215,7 +215,7 @@ static pfg_status batch_create(pfg_batch* b, uint32_t num_graphs, const uint32_t
         if (st != PFG_OK) return st;
         B_CUDA(cudaMemsetAsync(b->d_hubs, 0, (size_t)b->hub_cap * sizeof(HubRec), b->stream));
     }
-    B_CUDA(cudaMemsetAsync(b->d_ring, 0xFF, ring * 4, b->stream));
+    B_CUDA(cudaMemsetAsync(b->d_ring, 0xFF, ring * 8, b->stream));
     B_CUDA(cudaMemsetAsync(b->d_aq, 0, AQ_WORDS * 4, b->stream));
     for (int i = 0; i < 3; ++i) B_CUDA(cudaMemsetAsync(b->d_stamp[i], 0, S * 4, b->stream));
     B_CUDA(cudaMallocHost((void**)&b->h_ctl_init, sizeof(Ctl)));
@@ -406,7 +406,7 @@ static pfg_status batch_complete(pfg_batch* b, int mode, u32 delta, pfg_stats* s
         case DS_NOT_CONVERGED: return set_error(PFG_ERR_NOT_CONVERGED, "batch did not converge");
         case DS_TIMEOUT:
             // the next run must find the ring empty
-            cudaMemsetAsync(b->d_ring, 0xFF, ((u64)b->ring_mask + 1) * 4, b->stream);
+            cudaMemsetAsync(b->d_ring, 0xFF, ((u64)b->ring_mask + 1) * 8, b->stream);
             cudaMemsetAsync(b->d_aq, 0, AQ_WORDS * 4, b->stream);
             cudaStreamSynchronize(b->stream);
             return set_error(PFG_ERR_DEVICE_TIMEOUT, "device-side wait timed out: %s made no progress for %llu ms",

@@ -53,7 +53,9 @@ enum RingCounter : u32 { AQ_HEAD = 0, AQ_TAIL = 32, AQ_DONE = 64, AQ_BUSY = 96, 
 // CTA that waits (for work, or at the barrier after leaving a drain) measures its
 // time limit from the last change of the heartbeat, so a long but progressing
 // drain (one CTA walking a long chain) never reads as a hang.
-constexpr u32 RING_EMPTY = 0xFFFFFFFFu;  // a free ring slot
+// A ring entry is (distance the vertex was queued with) << 32 | state index;
+// RING_FREE marks a free slot (no entry has index 2^32 - 1 and distance INF).
+constexpr unsigned long long RING_FREE = ~0ull;
 
 // Grid tier of the hybrid mapping: an item whose selected arcs exceed
 // RunParams::hub_min is published as a hub record, and any CTA claims chunks
@@ -211,11 +213,13 @@ struct RunParams {
     u32 eager_max_items;  // ... only in rounds whose input has at most this many items
     const PolicyNet* net;
     u64 timeout_ns;    // bound on every device-side wait
-    // Asynchronous buckets (ring != nullptr): inside a bucket, vertices claimed
-    // for the window go to a ring of ring_mask + 1 slots (RING_EMPTY when free)
-    // and any CTA pulls them as soon as they are written; the grid barrier runs
-    // once per bucket instead of once per relaxation round.
-    u32* ring;
+    // Asynchronous buckets (ring != nullptr): inside a bucket, every improvement
+    // of a vertex into the window queues an entry (state index, new distance) in
+    // the improving CTA's claimed list or in a ring of ring_mask + 1 slots
+    // (RING_FREE when free), and any CTA pulls ring entries as soon as they are
+    // written; the grid barrier runs once per bucket instead of once per
+    // relaxation round.
+    unsigned long long* ring;
     u32 ring_mask;
     u32* aq;           // ring counters, see RingCounter
     int test_absent_cta;  // test hook: CTA 0 leaves at once, so every barrier wait runs out
@@ -249,6 +253,11 @@ __device__ __forceinline__ u32 ld_acquire(const u32* p) {
     return v;
 }
 __device__ __forceinline__ u64 vload64(const u64* p) { return *(const volatile u64*)p; }
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 
 // Records that the wait at `site` ran out of time (the first such wait names
 // the site) and ends the run with DS_TIMEOUT.
@@ -330,17 +339,18 @@ __device__ __forceinline__ void queue_push(u32* q, u32* tail, u32 item) {
 // by the consumer of position i - (ring_mask + 1); the compare-and-swap makes
 // a writer that catches up with a slow consumer wait (bounded) instead of
 // overwriting an unread item. Returns false if that wait timed out.
-__device__ __forceinline__ bool ring_push(u32* ring, u32 mask_bits, u32* tail, u32 item, u64 timeout_ns) {
+__device__ __forceinline__ bool ring_push(unsigned long long* ring, u32 mask_bits, u32* tail, unsigned long long item,
+                                          u64 timeout_ns) {
     const unsigned mask = __activemask();
     const int lane = threadIdx.x & 31;
     const int leader = __ffs(mask) - 1;
     u32 base = 0;
     if (lane == leader) base = atomicAdd(tail, (u32)__popc(mask));
     base = __shfl_sync(mask, base, leader);
-    u32* slot = ring + ((base + __popc(mask & ((1u << lane) - 1u))) & mask_bits);
-    if (atomicCAS(slot, RING_EMPTY, item) == RING_EMPTY) return true;
+    unsigned long long* slot = ring + ((base + __popc(mask & ((1u << lane) - 1u))) & mask_bits);
+    if (atomicCAS(slot, RING_FREE, item) == RING_FREE) return true;
     const u64 t0 = global_timer_ns();
-    while (atomicCAS(slot, RING_EMPTY, item) != RING_EMPTY) {
+    while (atomicCAS(slot, RING_FREE, item) != RING_FREE) {
         if (global_timer_ns() - t0 > timeout_ns) return false;
         __nanosleep(64);
     }

@@ -72,7 +72,7 @@ struct pfg_solver {
     u32* d_q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // near0, near1, far0, far1, R
     u32* d_stamp[3] = {nullptr, nullptr, nullptr};                // near, far, R
     u32* d_naive[2] = {nullptr, nullptr};
-    u32* d_ring = nullptr;      // ring queue of asynchronous buckets [ring_mask + 1], RING_EMPTY when idle
+    unsigned long long* d_ring = nullptr;  // ring queue of asynchronous buckets [ring_mask + 1], RING_FREE when idle
     u32 ring_mask = 0;
     u32* d_aq = nullptr;        // ring counters [AQ_WORDS]
     pfg::HubRec* d_hubs = nullptr;  // hub records of the grid tier [hub_cap]

@@ -23,6 +23,7 @@
 #include "pfg_common.cuh"
 #include "pfg_kernels.h"
 
+#include <atomic>
 #include <cstdio>
 
 namespace pfg {
@@ -59,6 +60,7 @@ struct Coop {
     u64 ub[MAX_BS];
     u32 wsum[32];
     u32 cl[CL_CAP];  // near vertices claimed by this CTA (circular: position i is cl[i % CL_CAP])
+    u32 cl_d[CL_CAP];  // asynchronous buckets: the distance each entry was queued with
     u32 cl_n;        // positions appended (may run past cl_head + CL_CAP; the excess went to a global queue)
     u32 cl_head;     // first position not yet taken (rounds: always 0; asynchronous buckets: advances)
     u32 cl_base;
@@ -157,9 +159,10 @@ __device__ __forceinline__ u32 light_end(const uint2* adj, u32 r0, u32 r1, u32 d
 // (eager sub-rounds) and flushed to the global near queue at the end of the
 // round; only overflow goes to the global queue directly.
 // Appends gv, which this thread has just claimed (near: for the current
-// window; else: for the far pile), to the claimed list, the ring, or a queue.
-__device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, u32 gv, bool near, u32 inst,
-                                             Local& L, Coop* cl) {
+// window; else: for the far pile), to the claimed list, the ring, or a queue;
+// nd is its new distance (carried by entries of asynchronous buckets).
+__device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, u32 gv, u32 nd, bool near,
+                                             u32 inst, Local& L, Coop* cl) {
     Ctl* c = p.ctl;
     L.pushes++;
     if (!near) {
@@ -171,11 +174,13 @@ __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, 
         const u32 slot = atomicAdd(&cl->cl_n, 1u);
         if (slot - cl->cl_head < CL_CAP) {
             cl->cl[slot & (CL_CAP - 1u)] = gv;
+            cl->cl_d[slot & (CL_CAP - 1u)] = nd;
             return;
         }
     }
     if (s.async_bkt) {
-        if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, gv, p.timeout_ns)) flag_timeout(c, WS_RING_PUSH);
+        if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, ((unsigned long long)nd << 32) | gv, p.timeout_ns))
+            flag_timeout(c, WS_RING_PUSH);
         return;
     }
     const u32 out = s.in_buf ^ 1u;
@@ -184,8 +189,8 @@ __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, 
 
 // After gv's distance was lowered to a value of key `key`: flag it (prefix-scan
 // compaction) or claim it for the window / the far pile and queue it.
-__device__ __forceinline__ void after_improve(const RunParams& p, const Snap& s, u32 gv, u64 key, u32 inst,
-                                              Local& L, Coop* cl) {
+__device__ __forceinline__ void after_improve(const RunParams& p, const Snap& s, u32 gv, u64 key, u32 nd,
+                                              u32 inst, Local& L, Coop* cl) {
     L.updates++;
     if (p.prefix_scan) {  // flag only; the COMPACT round builds the next frontier
         p.near_stamp[gv] = s.near_epoch;
@@ -194,25 +199,80 @@ __device__ __forceinline__ void after_improve(const RunParams& p, const Snap& s,
     }
     const bool near = key < s.hi;
     if (!near) L.fmin = key < L.fmin ? key : L.fmin;
+    if (near && s.async_bkt) {
+        // Asynchronous bucket: no claim. Every strict improvement queues an
+        // entry with the distance it set; an entry whose vertex has been
+        // improved again by the time it is taken is skipped (the later
+        // improvement queued its own), so each value a vertex reaches in the
+        // window is relaxed once, without a claim exchange on the push or a
+        // release and fence on the take.
+        push_claimed(p, s, gv, nd, true, inst, L, cl);
+        return;
+    }
     if (claim_stamp(near ? p.near_stamp : p.far_stamp, gv, near ? s.near_epoch : s.far_epoch))
-        push_claimed(p, s, gv, near, inst, L, cl);
+        push_claimed(p, s, gv, nd, near, inst, L, cl);
+}
+
+// Candidate distance nd and key of arc (u -> v, w) from du; false for a
+// padding arc, a distance that leaves 32 bits, or (A*) a pruned key.
+template <bool ASTAR>
+__device__ __forceinline__ bool arc_candidate(const RunParams& p, u32 du, u64 ub, u32 inst, u32 v, u32 w,
+                                              Local& L, u64& nd, u64& key) {
+    if (w == PAD_W) return false;
+    L.edges++;
+    nd = (u64)du + w;
+    if (nd >= INF32) return false;
+    key = nd;
+    if constexpr (ASTAR) {
+        key = astar_key(p, inst, v, nd);
+        if (key >= ub) return false;  // f(v) >= dist[target]: cannot improve the answer
+    }
+    return true;
 }
 
 template <bool ASTAR, int AM>
 __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32 u, u32 du,
                                           u32 ib, u64 ub, u32 inst, u32 v, u32 w, Local& L, Coop* cl) {
-    if (w == PAD_W) return;
-    L.edges++;
-    const u64 nd = (u64)du + w;
-    if (nd >= INF32) return;
-    u64 key = nd;
-    if constexpr (ASTAR) {
-        key = astar_key(p, inst, v, nd);
-        if (key >= ub) return;  // f(v) >= dist[target]: cannot improve the answer
-    }
+    u64 nd = 0, key = 0;
+    if (!arc_candidate<ASTAR>(p, du, ub, inst, v, w, L, nd, key)) return;
     const u32 gv = ib + v;
     if (!relax_state<AM>(p.state + gv, (u32)nd, u, L.atomics)) return;
-    after_improve(p, s, gv, key, inst, L, cl);
+    after_improve(p, s, gv, key, (u32)nd, inst, L, cl);
+}
+
+// Two arcs of one lane relaxed together: both state updates are issued before
+// either result is used, so their L2 round trips overlap (same outcome as two
+// relax_arc calls in a row).
+template <bool ASTAR, int AM>
+__device__ __forceinline__ void relax_arc_pair(const RunParams& p, const Snap& s, bool va, u32 ua, u32 dua,
+                                               u32 iba, u64 uba, u32 insta, uint2 aa, bool vb, u32 ub2, u32 dub,
+                                               u32 ibb, u64 ubb, u32 instb, uint2 ab, Local& L, Coop* cl) {
+    u64 nda = 0, keya = 0, ndb = 0, keyb = 0;
+    const bool ga = va && arc_candidate<ASTAR>(p, dua, uba, insta, aa.x, aa.y, L, nda, keya);
+    const bool gb = vb && arc_candidate<ASTAR>(p, dub, ubb, instb, ab.x, ab.y, L, ndb, keyb);
+    const u32 gva = iba + aa.x, gvb = ibb + ab.x;
+    bool ia, ibt;
+    if constexpr (AM == 1) {
+        ia = ga && relax_state<1>(p.state + gva, (u32)nda, ua, L.atomics);
+        ibt = gb && relax_state<1>(p.state + gvb, (u32)ndb, ub2, L.atomics);
+    } else {
+        const u64 nva = pack_state((u32)nda, ua), nvb = pack_state((u32)ndb, ub2);
+        bool ta = ga, tb = gb;
+        if constexpr (AM == 0) {  // read before atomic: both reads in flight, then both atomics
+            const u64 ca = ga ? ld_state(p.state + gva) : 0ull;
+            const u64 cb = gb ? ld_state(p.state + gvb) : 0ull;
+            ta = ga && ca > nva;
+            tb = gb && cb > nvb;
+        }
+        unsigned long long oa = ~0ull, ob = ~0ull;
+        if (ta) oa = atomicMin((unsigned long long*)(p.state + gva), (unsigned long long)nva);
+        if (tb) ob = atomicMin((unsigned long long*)(p.state + gvb), (unsigned long long)nvb);
+        L.atomics += (ta ? 1u : 0u) + (tb ? 1u : 0u);
+        ia = ta && st_dist(oa) > (u32)nda;
+        ibt = tb && st_dist(ob) > (u32)ndb;
+    }
+    if (ia) after_improve(p, s, gva, keya, (u32)nda, insta, L, cl);
+    if (ibt) after_improve(p, s, gvb, keyb, (u32)ndb, instb, L, cl);
 }
 
 // Thread tier: one thread walks its own arcs [eb, ee) with 128-bit loads
@@ -253,16 +313,20 @@ __device__ __forceinline__ void decode_item(const RunParams& p, u32 gi, u32& ins
 // items of a later bucket are carried to the next far pile here. On true,
 // [eb, ee) is the arc range of the round kind (light prefix / heavy suffix).
 // The row bounds are loaded together with the state word (one round trip),
-// or passed in (pre) by a caller that loaded them earlier.
+// or passed in (pre) by a caller that loaded them earlier. An entry of an
+// asynchronous bucket passes the distance it was queued with (want): it is
+// stale, and skipped, if the vertex has been improved since.
 template <bool ASTAR>
 __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32 gi, int kind,
                                           Local& L, u32& u, u32& ib, u32& du, u64& ub, u32& inst,
-                                          u32& eb, u32& ee, bool pre = false, u32 pr0 = 0u, u32 pr1 = 0u) {
+                                          u32& eb, u32& ee, bool pre = false, u32 pr0 = 0u, u32 pr1 = 0u,
+                                          u32 want = INF32) {
     Ctl* c = p.ctl;
     u32 rb;
     decode_item(p, gi, inst, ib, rb, u);
     const u32 r0 = pre ? pr0 : __ldg(p.prow + rb + u), r1 = pre ? pr1 : __ldg(p.prow + rb + u + 1);
     du = st_dist(ld_state(p.state + gi));
+    if (want != INF32 && du != want) return false;
     bool act = du != INF32;
     u64 key = du;
     if constexpr (ASTAR) {
@@ -385,7 +449,35 @@ __device__ __forceinline__ void relax_items_warp(const RunParams& p, const Snap&
     }
     const u32 total = __shfl_sync(FULL, x, 31);
     const u32 off = x - sz;
-    for (u32 j0 = 0; j0 < total; j0 += 32) {  // warp-uniform
+    u32 j0 = 0;
+    // More than 32 arcs left: two per lane, relaxed together (one dependent
+    // chain of loads and atomics instead of two in a row).
+    while (j0 + 32u < total) {  // warp-uniform; j0 may pass total when it ends
+        const u32 ja = j0 + lane, jb = ja + 32u;
+        u32 loa = 0, lob = 0;
+#pragma unroll
+        for (u32 step = 16; step > 0; step >>= 1) {
+            if (__shfl_sync(FULL, off, loa + step) <= ja) loa += step;
+            if (__shfl_sync(FULL, off, lob + step) <= jb) lob += step;
+        }
+        const u32 au = __shfl_sync(FULL, u, loa), adu = __shfl_sync(FULL, du, loa);
+        const u32 aib = __shfl_sync(FULL, ib, loa), ainst = __shfl_sync(FULL, inst, loa);
+        const u32 aeb = __shfl_sync(FULL, eb, loa) + (ja - __shfl_sync(FULL, off, loa));
+        const u32 bu = __shfl_sync(FULL, u, lob), bdu = __shfl_sync(FULL, du, lob);
+        const u32 bib = __shfl_sync(FULL, ib, lob), binst = __shfl_sync(FULL, inst, lob);
+        const u32 beb = __shfl_sync(FULL, eb, lob) + (jb - __shfl_sync(FULL, off, lob));
+        u64 aub = ~0ull, bub = ~0ull;
+        if constexpr (ASTAR) {
+            aub = __shfl_sync(FULL, ub, loa);
+            bub = __shfl_sync(FULL, ub, lob);
+        }
+        const bool vb = jb < total;
+        const uint2 aa = __ldg(p.adj + aeb);
+        const uint2 ab = vb ? __ldg(p.adj + beb) : make_uint2(0u, PAD_W);
+        relax_arc_pair<ASTAR, AM>(p, s, true, au, adu, aib, aub, ainst, aa, vb, bu, bdu, bib, bub, binst, ab, L, cl);
+        j0 += 64u;
+    }
+    for (; j0 < total; j0 += 32) {  // warp-uniform
         const u32 j = j0 + lane;
         // owner = last lane whose offset is <= j (empty items repeat offsets)
         u32 lo = 0;
@@ -585,7 +677,7 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
 
 // ---------------------------------------------------------------------------
 // Asynchronous drain of a bucket (phase ASYNC). Each CTA works through its own
-// claimed list first (the near vertices its relaxations claimed, kept in shared
+// claimed list first (the entries its relaxations queued, kept in shared
 // memory, up to one block of items per pass), so a wavefront advances hop by
 // hop without any global queue traffic. Work moves between CTAs through the
 // ring: a CTA spills the newest part of its backlog there when other CTAs are
@@ -600,8 +692,10 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
 // gave it claimed items as done, and returns it only after the pushes of its
 // last pass were performed, so the test never passes while work exists.
 //
-// A popped vertex releases its claim before its state is read (the fence
-// orders the two), so an improvement that lands after the read queues it again.
+// Entries carry the distance they were queued with; a popped entry whose
+// vertex has a smaller distance by now is stale and skipped. Every strict
+// improvement queues an entry, so the entry of the value a vertex keeps is
+// always relaxed, whatever order the CTAs run in.
 // ---------------------------------------------------------------------------
 template <bool ASTAR, int AM, int MAP>
 __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& cs, bool busy_held) {
@@ -720,11 +814,12 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
             // the newest part of the backlog goes to the ring for idle CTAs
             const u32 from = s_spill_from, base = s_spill_base;
             for (u32 i = threadIdx.x; i < spill; i += BS) {
-                u32* slot = p.ring + ((base + i) & p.ring_mask);
-                const u32 gi = cs.cl[(from + i) & CLM];
-                if (atomicCAS(slot, RING_EMPTY, gi) != RING_EMPTY) {
+                unsigned long long* slot = p.ring + ((base + i) & p.ring_mask);
+                const unsigned long long ent = ((unsigned long long)cs.cl_d[(from + i) & CLM] << 32) |
+                                               cs.cl[(from + i) & CLM];
+                if (atomicCAS(slot, RING_FREE, ent) != RING_FREE) {
                     const u64 t0 = global_timer_ns();
-                    while (atomicCAS(slot, RING_EMPTY, gi) != RING_EMPTY) {
+                    while (atomicCAS(slot, RING_FREE, ent) != RING_FREE) {
                         if (global_timer_ns() - t0 > p.timeout_ns) {
                             flag_timeout(c, WS_SPILL_SLOT);
                             break;
@@ -742,16 +837,16 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
         bool act = false;
         const u32 my = item_slot();
         if (my < n) {
-            u32 gi;
+            unsigned long long ent;
             if (src == 1u) {
-                gi = cs.cl[(h + my) & CLM];
+                ent = ((unsigned long long)cs.cl_d[(h + my) & CLM] << 32) | cs.cl[(h + my) & CLM];
             } else {
-                u32* slot = p.ring + ((h + my) & p.ring_mask);
-                gi = ld_relaxed(slot);
-                if (gi == RING_EMPTY) {
+                unsigned long long* slot = p.ring + ((h + my) & p.ring_mask);
+                ent = ld_relaxed64(slot);
+                if (ent == RING_FREE) {
                     // reserved by a producer that has not written it yet
                     const u64 t0 = global_timer_ns();
-                    while ((gi = ld_relaxed(slot)) == RING_EMPTY) {
+                    while ((ent = ld_relaxed64(slot)) == RING_FREE) {
                         if (global_timer_ns() - t0 > p.timeout_ns) {
                             flag_timeout(c, WS_RING_SLOT);
                             break;
@@ -759,15 +854,12 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
                         __nanosleep(32);
                     }
                 }
-                if (gi != RING_EMPTY) *slot = RING_EMPTY;
+                if (ent != RING_FREE) *slot = RING_FREE;
             }
-            if (gi != RING_EMPTY) {
-                u32 i0, b0, rb0, u0;
-                decode_item(p, gi, i0, b0, rb0, u0);
-                const u32 r0 = __ldg(p.prow + rb0 + u0), r1 = __ldg(p.prow + rb0 + u0 + 1);  // in flight across the fence
-                p.near_stamp[gi] = 0u;  // release the claim (epochs start at 1)
-                __threadfence();
-                act = take_item<ASTAR>(p, s, gi, K_LIGHT, L, u, ib, du, ub, inst, eb, ee, true, r0, r1);
+            if (ent != RING_FREE) {
+                const u32 gi = (u32)ent;
+                act = take_item<ASTAR>(p, s, gi, K_LIGHT, L, u, ib, du, ub, inst, eb, ee, false, 0u, 0u,
+                                       (u32)(ent >> 32));
                 if (MAP == 2 && act && p.hubs && ee - eb > p.hub_min && hub_publish(p, s, gi, eb, ee)) act = false;
             }
         }
@@ -1309,7 +1401,10 @@ __device__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, Ct
 template <bool ASTAR, int AM, int MAP>
 __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p) {
     __shared__ Snap s;
-    __shared__ Coop cs;
+    // the cooperative-mapping arrays and the claimed list live in dynamic shared
+    // memory (more than the 48 KB static limit)
+    extern __shared__ __align__(16) unsigned char pfg_dyn_smem[];
+    Coop& cs = *reinterpret_cast<Coop*>(pfg_dyn_smem);
     __shared__ Ctl sc;
     __shared__ u64 red[32];
     __shared__ u32 s_flag[3];
@@ -1421,6 +1516,22 @@ static const void* kernel_for(bool astar, int am, int map) {
     return astar ? (const void*)pick_am_map<true>(am, map) : (const void*)pick_am_map<false>(am, map);
 }
 
+// Dynamic shared memory of the persistent kernel (one Coop per CTA); the
+// opt-in above 48 KB is set once per instantiation and device (not a stream
+// operation, so launches inside a stream capture need nothing more).
+static cudaError_t allow_coop_smem(bool astar, int am, int map) {
+    static std::atomic<unsigned> done[64];  // bit (astar, am, map) per device
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned bit = 1u << ((astar ? 9 : 0) + 3 * am + map);
+    if (dev < 64 && (done[dev].load() & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel_for(astar, am, map), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(Coop));
+    if (e == cudaSuccess && dev < 64) done[dev].fetch_or(bit);
+    return e;
+}
+
 cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, int block,
                               int grid, cudaStream_t st) {
     // Cooperative attribute: the driver refuses a grid that cannot be fully
@@ -1428,7 +1539,12 @@ cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, i
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = 0;
+    if (am < 0 || am > 2) am = 0;
+    if (map < 0 || map > 2) map = 2;
+    const void* k = kernel_for(astar, am, map);
+    const cudaError_t ea = allow_coop_smem(astar, am, map);
+    if (ea != cudaSuccess) return ea;
+    cfg.dynamicSmemBytes = sizeof(Coop);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -1436,13 +1552,16 @@ cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, i
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     void* args[] = {(void*)&p};
-    return cudaLaunchKernelExC(&cfg, kernel_for(astar, am, map), args);
+    return cudaLaunchKernelExC(&cfg, k, args);
 }
 
 int persistent_blocks_per_sm(bool astar, int am, int map, int block) {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel_for(astar, am, map), block, 0) !=
-        cudaSuccess) {
+    if (am < 0 || am > 2) am = 0;
+    if (map < 0 || map > 2) map = 2;
+    const void* k = kernel_for(astar, am, map);
+    if (allow_coop_smem(astar, am, map) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block, sizeof(Coop)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }

@@ -449,7 +449,7 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
     v->steps++;
     if (v->h_rd->status == DS_TIMEOUT) {
         // the next step must find the ring empty
-        cudaMemsetAsync(s->d_ring, 0xFF, ((u64)s->ring_mask + 1) * 4, st);
+        cudaMemsetAsync(s->d_ring, 0xFF, ((u64)s->ring_mask + 1) * 8, st);
         cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, st);
         cudaStreamSynchronize(st);
         return set_error(PFG_ERR_DEVICE_TIMEOUT, "device-side wait timed out: %s made no progress for %llu ms",

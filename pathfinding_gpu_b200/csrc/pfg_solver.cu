@@ -293,12 +293,13 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
         TRY(s->dalloc(&s->d_naive[i], words));
         TRYC(cudaMemsetAsync(s->d_naive[i], 0, words * 4, s->stream));
     }
-    // Ring of the asynchronous buckets: a power of two >= K*n slots, so the
-    // live items (at most one per state word) always fit.
+    // Ring of the asynchronous buckets: entries are queued per strict
+    // improvement (several may be in flight for one vertex), so it has a power
+    // of two >= 2 K n slots (at most 2^32: positions are u32 counters).
     u64 ring = 1024;
-    while (ring < Kn) ring <<= 1;
+    while (ring < 2 * Kn && ring < (1ull << 32)) ring <<= 1;
     TRY(s->dalloc(&s->d_ring, ring));
-    TRYC(cudaMemsetAsync(s->d_ring, 0xFF, ring * 4, s->stream));
+    TRYC(cudaMemsetAsync(s->d_ring, 0xFF, ring * 8, s->stream));
     s->ring_mask = (u32)(ring - 1);
     TRY(s->dalloc(&s->d_aq, (u64)AQ_WORDS));
     TRYC(cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, s->stream));
@@ -584,7 +585,7 @@ static pfg_status complete_run(pfg_solver* s, pfg_stats* stats_out) {
         // A wait gave up: reset the naive masks and the ring so the next run starts clean.
         const u64 words = (u64)s->n / 32 + 1;
         for (int i = 0; i < 2; ++i) cudaMemsetAsync(s->d_naive[i], 0, words * 4, s->stream);
-        cudaMemsetAsync(s->d_ring, 0xFF, ((u64)s->ring_mask + 1) * 4, s->stream);
+        cudaMemsetAsync(s->d_ring, 0xFF, ((u64)s->ring_mask + 1) * 8, s->stream);
         cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, s->stream);
         cudaStreamSynchronize(s->stream);
         return fail(PFG_ERR_DEVICE_TIMEOUT, "device-side wait timed out: %s made no progress for %llu ms",
