@@ -9,7 +9,9 @@ step time (the reference's TEPS definition, src/main.cpp:209-213, aggregated
 over the batch).
 
   value  device time of the step with the graph, sources and working set resident
-         in HBM (CUDA events on the solver's stream, L2 flushed between steps)
+         in HBM (CUDA events on the solver's stream, L2 flushed between steps); the
+         launch shape (threads per CTA x CTAs per SM) is the fastest of the
+         autotuner's candidates on this workload, timed before the warm-up
   e2e    the same step through the C ABI as the reference's multiSource with distOut
          (pfg_run + pfg_copy_dist): H2D of the K sources from pinned memory, the run,
          the distances of the K*n states split from the packed words on the device and
@@ -187,6 +189,23 @@ def run_ours(args, D):
 
     d_srcs = torch.from_numpy(srcs.astype(np.int32)).to(f"cuda:{D.local}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{D.local}")
+
+    # Launch shape: the autotuner's launch-shape candidates timed on this
+    # workload before the warm-up (median of 3 runs each, L2 flushed); Delta
+    # stays the automatic value and the schedule the default.
+    from dataclasses import replace
+    from pathfinding_gpu_b200.autotune import LAUNCH_SHAPES
+    shape_ms = {}
+    for bsz, bps in LAUNCH_SHAPES:
+        trial = replace(opt, blockSize=bsz, blocksPerSM=bps)
+        ts = []
+        for _ in range(3):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ts.append(solver.run_state(srcs, trial, copy=False)[1])
+        shape_ms[f"{bsz}x{bps}"] = round(statistics.median(ts), 3)
+    bsz, bps = min(LAUNCH_SHAPES, key=lambda s: shape_ms[f"{s[0]}x{s[1]}"])
+    opt = replace(opt, blockSize=bsz, blocksPerSM=bps)
     copt = opt.to_c()
 
     def device_step():
@@ -270,7 +289,8 @@ def run_ours(args, D):
                             f"w=llround(100*U[1,1.5)), seed {SEED}",
                    "n": g.n, "m": g.m, "batch": K, "delta": stats0.delta, "algo": "DeltaStep",
                    "schedule": opt.schedule.name, "mapping": opt.mapping.name, "atomic": opt.atomic.name,
-                   "block": opt.blockSize, "l2": "flushed between steps (256 MB write)",
+                   "block": opt.blockSize, "ctas_per_sm": opt.blocksPerSM,
+                   "launch_shape_ms": shape_ms, "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"replicas x{D.world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 5), "traffic": traffic,

@@ -30,6 +30,7 @@ struct pfg_batch {
     std::vector<u32> g_n, g_m, g_rowbase;
     u32 maxw = 0;
     u32 max_deg = 0;
+    u32 row_stride = 0;  // ROW_ALIGN when every row of every graph has exactly ROW_ALIGN slots
     u64 hub_rows = 0;  // vertices with more than 256 arcs (all graphs)
     double avg_w = 0.0, avg_deg = 0.0;
     u64 max_states = 0;
@@ -125,6 +126,17 @@ static pfg_status batch_create(pfg_batch* b, uint32_t num_graphs, const uint32_t
         pfg_status st = validate_csr(rows[g], cols[g], ws[g], ns[g], ms[g], &mw);
         if (st != PFG_OK) return st;
         b->maxw = std::max(b->maxw, mw);
+        for (u32 u = 0; u < ns[g]; ++u) {
+            const u32 deg = rows[g][u + 1] - rows[g][u];
+            b->max_deg = std::max(b->max_deg, deg);
+            b->hub_rows += deg > 256u ? 1u : 0u;
+        }
+    }
+    // no row with more than 4 arcs in any graph: every row gets exactly 4 slots
+    // (row u of a graph starts at its first row + 4u; the kernel loads no prow)
+    const bool uniform_rows = b->max_deg <= ROW_ALIGN;
+    b->row_stride = uniform_rows ? ROW_ALIGN : 0u;
+    for (u32 g = 0; g < num_graphs; ++g) {
         for (u32 k = 0; k < ms[g]; ++k) w_sum += ws[g][k];
         m_total += ms[g];
         n_total += ns[g];
@@ -133,9 +145,7 @@ static pfg_status batch_create(pfg_batch* b, uint32_t num_graphs, const uint32_t
         for (u32 u = 0; u < ns[g]; ++u) {
             pr[u] = (u32)pad_total;
             const u32 deg = rows[g][u + 1] - rows[g][u];
-            b->max_deg = std::max(b->max_deg, deg);
-            b->hub_rows += deg > 256u ? 1u : 0u;
-            pad_total += (u64)((deg + ROW_ALIGN - 1) / ROW_ALIGN) * ROW_ALIGN;
+            pad_total += uniform_rows ? ROW_ALIGN : (u64)((deg + ROW_ALIGN - 1) / ROW_ALIGN) * ROW_ALIGN;
         }
         pr[ns[g]] = (u32)pad_total;
         if (pad_total >= 0xFFFFFFF0ull) return set_error(PFG_ERR_INVALID_GRAPH, "padded arcs of the batch exceed 2^32");
@@ -321,6 +331,7 @@ static pfg_status batch_prepare(pfg_batch* b, const pfg_options* opt_in, RunPara
     memset(&p, 0, sizeof(p));
     p.adj = b->d_adj;
     p.prow = b->d_prow;
+    p.row_stride = b->row_stride;
     p.n = (u32)std::min<u64>(b->total_states, 0xFFFFFFFFull);
     p.maxw = b->maxw;
     p.avg_w = b->avg_w;

@@ -221,6 +221,10 @@ struct RunParams {
     // relaxation round.
     unsigned long long* ring;
     u32 ring_mask;
+    // ROW_ALIGN when every row of the graph(s) occupies exactly ROW_ALIGN slots
+    // (no row has more arcs): row u of a graph starts at prow[first row] +
+    // ROW_ALIGN * u, so an item's arcs are addressed without loading prow.
+    u32 row_stride;
     u32* aq;           // ring counters, see RingCounter
     int test_absent_cta;  // test hook: CTA 0 leaves at once, so every barrier wait runs out
     HubRec* hubs;      // hub records (nullptr: no row of the graph is long enough)

@@ -55,6 +55,7 @@ struct pfg_solver {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     u32 n = 0, m = 0, K = 1, maxw = 0;
     u32 max_deg = 0;            // largest out-degree
+    u32 row_stride = 0;         // ROW_ALIGN when every row has exactly ROW_ALIGN slots, else 0
     u64 hub_rows = 0;           // vertices with more than 256 arcs
     u64 m_pad = 0;
     double hscale = 0.0, avg_w = 0.0, avg_deg = 0.0;

@@ -324,7 +324,20 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
     Ctl* c = p.ctl;
     u32 rb;
     decode_item(p, gi, inst, ib, rb, u);
-    const u32 r0 = pre ? pr0 : __ldg(p.prow + rb + u), r1 = pre ? pr1 : __ldg(p.prow + rb + u + 1);
+    u32 r0, r1;
+    if (pre) {
+        r0 = pr0;
+        r1 = pr1;
+    } else if (p.row_stride) {
+        // fixed-stride rows: the arc block is known now, so it is fetched into
+        // L1 while the state word is read (the relaxation's loads then hit)
+        r0 = (rb ? __ldg(p.prow + rb) : 0u) + ROW_ALIGN * u;
+        r1 = r0 + ROW_ALIGN;
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(p.adj + r0));
+    } else {
+        r0 = __ldg(p.prow + rb + u);
+        r1 = __ldg(p.prow + rb + u + 1);
+    }
     du = st_dist(ld_state(p.state + gi));
     if (want != INF32 && du != want) return false;
     bool act = du != INF32;
@@ -559,7 +572,7 @@ __device__ __forceinline__ bool hub_publish(const RunParams& p, const Snap& s, u
 // s_hub[1] is the record and [s_hub[3], s_hub[4]) the chunk. Called by every
 // thread of the CTA.
 template <bool ASTAR, int AM>
-__device__ bool hub_chunk(const RunParams& p, const Snap& s, Local& L, Coop* cl, u32* s_hub) {
+__device__ __forceinline__ bool hub_chunk(const RunParams& p, const Snap& s, Local& L, Coop* cl, u32* s_hub) {
     __shared__ u32 s_u, s_du, s_ib, s_inst;
     __shared__ u64 s_ub;
     if (threadIdx.x == 0) {
@@ -603,7 +616,7 @@ __device__ bool hub_chunk(const RunParams& p, const Snap& s, Local& L, Coop* cl,
 }
 
 template <bool ASTAR, int AM, int MAP>
-__device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u32 count, int kind,
+__device__ __forceinline__ void round_items(const RunParams& p, const Snap& s, const u32* in, u32 count, int kind,
                             Local& L, Coop& cs) {
     const u32 BS = blockDim.x;
     // Hybrid mapping keeps claimed near vertices in shared memory (see relax_arc).
@@ -698,7 +711,7 @@ __device__ void round_items(const RunParams& p, const Snap& s, const u32* in, u3
 // always relaxed, whatever order the CTAs run in.
 // ---------------------------------------------------------------------------
 template <bool ASTAR, int AM, int MAP>
-__device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& cs, bool busy_held) {
+__device__ __forceinline__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& cs, bool busy_held) {
     __shared__ u32 s_src, s_h, s_n, s_spill, s_spill_from, s_spill_base, s_busy, s_idle;
     __shared__ u32 s_hub[8];
     constexpr u32 CLM = CL_CAP - 1u;
@@ -890,7 +903,7 @@ __device__ void async_drain(const RunParams& p, const Snap& s, Local& L, Coop& c
 // (Harish & Narayanan; reference naiveRelaxKernel, src/gpu_kernels.cuh:297-329).
 // ---------------------------------------------------------------------------
 template <bool ASTAR, int AM>
-__device__ void round_naive(const RunParams& p, const Snap& s, Local& L) {
+__device__ __forceinline__ void round_naive(const RunParams& p, const Snap& s, Local& L) {
     u32* mask_in = p.naive_mask[s.naive_in];
     u32* mask_out = p.naive_mask[s.naive_in ^ 1u];
     Ctl* c = p.ctl;
@@ -1319,7 +1332,7 @@ __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, float* s_fe
 // p.timeout_ns, or sees an error status, stops waiting and the kernel winds
 // down; no wait is unbounded.
 // ---------------------------------------------------------------------------
-__device__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, Ctl& sc, u32* s_flag,
+__device__ __forceinline__ void grid_barrier(const RunParams& p, Snap& s, Local& L, u64* red, Ctl& sc, u32* s_flag,
                              float* s_feat, float* act0, float* act1) {
     __syncthreads();
     Ctl* c = p.ctl;

@@ -390,6 +390,7 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
     memset(&p, 0, sizeof(p));
     p.adj = s->d_adj;
     p.prow = s->d_prow;
+    p.row_stride = s->row_stride;
     p.x = s->d_x;
     p.y = s->d_y;
     p.n = n;
