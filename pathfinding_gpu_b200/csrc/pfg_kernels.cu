@@ -49,22 +49,24 @@ struct Local {
 
 constexpr u32 CL_CAP = 2048;  // claimed-list entries per CTA (hybrid mapping)
 
-// Shared memory of the edge-balanced hybrid mapping.
+// Per-CTA shared memory of the hybrid mapping (dynamic shared memory). The
+// edge-balanced mapping's per-thread arrays follow the struct, sized by the
+// launch's block size (coop_bytes), so a small CTA keeps the rest of the
+// SM's 228 KB as L1 for the arc, coordinate and row-offset loads.
 struct Coop {
-    u32 off[MAX_BS + 1];
-    u32 eb[MAX_BS];
-    u32 u[MAX_BS];
-    u32 du[MAX_BS];
-    u32 ib[MAX_BS];
-    u32 inst[MAX_BS];
-    u64 ub[MAX_BS];
     u32 wsum[32];
     u32 cl[CL_CAP];  // near vertices claimed by this CTA (circular: position i is cl[i % CL_CAP])
     u32 cl_d[CL_CAP];  // asynchronous buckets: the distance each entry was queued with
     u32 cl_n;        // positions appended (may run past cl_head + CL_CAP; the excess went to a global queue)
     u32 cl_head;     // first position not yet taken (rounds: always 0; asynchronous buckets: advances)
     u32 cl_base;
+    u32 pad;
 };
+static_assert(sizeof(Coop) % 16 == 0, "the per-thread arrays after Coop need 16-byte alignment");
+
+// Bytes of dynamic shared memory for a CTA of `block` threads: Coop, then
+// u64 ub[block], u32 off[block + 1], eb[block], u[block], du[block], ib[block], inst[block].
+__host__ __device__ constexpr size_t coop_bytes(u32 block) { return sizeof(Coop) + (size_t)block * 32u + 4u; }
 
 // ---------------------------------------------------------------------------
 // Block-wide exclusive scan (warp shuffles + one pass over warp totals).
@@ -393,14 +395,21 @@ __device__ __forceinline__ void relax_chunk_edges(const RunParams& p, const Snap
     const u32 sz = act ? ee - eb : 0u;
     const u32 off = block_exclusive_scan(sz, cs.wsum, total);
     if (total == 0) return;  // block-uniform
-    cs.off[threadIdx.x] = off;
-    cs.eb[threadIdx.x] = eb;
-    cs.u[threadIdx.x] = u;
-    cs.du[threadIdx.x] = du;
-    cs.ib[threadIdx.x] = ib;
-    cs.ub[threadIdx.x] = ub;
-    cs.inst[threadIdx.x] = inst;
-    if (threadIdx.x == 0) cs.off[BS] = total;
+    u64* c_ub = reinterpret_cast<u64*>(&cs + 1);
+    u32* c_off = reinterpret_cast<u32*>(c_ub + BS);
+    u32* c_eb = c_off + BS + 1;
+    u32* c_u = c_eb + BS;
+    u32* c_du = c_u + BS;
+    u32* c_ib = c_du + BS;
+    u32* c_inst = c_ib + BS;
+    c_off[threadIdx.x] = off;
+    c_eb[threadIdx.x] = eb;
+    c_u[threadIdx.x] = u;
+    c_du[threadIdx.x] = du;
+    c_ib[threadIdx.x] = ib;
+    c_ub[threadIdx.x] = ub;
+    c_inst[threadIdx.x] = inst;
+    if (threadIdx.x == 0) c_off[BS] = total;
     __syncthreads();
     for (u32 j = threadIdx.x; j < total; j += BS) {
         // owner = last slot with off <= j (zero-size slots repeat offsets, the
@@ -409,11 +418,11 @@ __device__ __forceinline__ void relax_chunk_edges(const RunParams& p, const Snap
 #pragma unroll
         for (u32 step = MAX_BS / 2; step > 0; step >>= 1) {
             const u32 cand = lo + step;
-            if (cand < BS && cs.off[cand] <= j) lo = cand;
+            if (cand < BS && c_off[cand] <= j) lo = cand;
         }
-        const u32 e = cs.eb[lo] + (j - cs.off[lo]);
+        const u32 e = c_eb[lo] + (j - c_off[lo]);
         const uint2 a = __ldg(p.adj + e);
-        relax_arc<ASTAR, AM>(p, s, cs.u[lo], cs.du[lo], cs.ib[lo], cs.ub[lo], cs.inst[lo], a.x, a.y, L, cl);
+        relax_arc<ASTAR, AM>(p, s, c_u[lo], c_du[lo], c_ib[lo], c_ub[lo], c_inst[lo], a.x, a.y, L, cl);
     }
     __syncthreads();
 }
@@ -1540,7 +1549,7 @@ static cudaError_t allow_coop_smem(bool astar, int am, int map) {
     const unsigned bit = 1u << ((astar ? 9 : 0) + 3 * am + map);
     if (dev < 64 && (done[dev].load() & bit)) return cudaSuccess;
     e = cudaFuncSetAttribute(kernel_for(astar, am, map), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(Coop));
+                             (int)coop_bytes(MAX_BS));
     if (e == cudaSuccess && dev < 64) done[dev].fetch_or(bit);
     return e;
 }
@@ -1557,7 +1566,7 @@ cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, i
     const void* k = kernel_for(astar, am, map);
     const cudaError_t ea = allow_coop_smem(astar, am, map);
     if (ea != cudaSuccess) return ea;
-    cfg.dynamicSmemBytes = sizeof(Coop);
+    cfg.dynamicSmemBytes = coop_bytes((u32)block);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -1574,7 +1583,7 @@ int persistent_blocks_per_sm(bool astar, int am, int map, int block) {
     if (map < 0 || map > 2) map = 2;
     const void* k = kernel_for(astar, am, map);
     if (allow_coop_smem(astar, am, map) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block, sizeof(Coop)) != cudaSuccess) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block, coop_bytes((u32)block)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
