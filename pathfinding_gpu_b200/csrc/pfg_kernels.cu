@@ -194,6 +194,11 @@ __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, 
 __device__ __forceinline__ void after_improve(const RunParams& p, const Snap& s, u32 gv, u64 key, u32 nd,
                                               u32 inst, Local& L, Coop* cl) {
     L.updates++;
+    if (p.mode == MODE_NAIVE) {  // Bellman-Ford sweep: the head is active in the next sweep
+        atomicOr(p.naive_mask[s.naive_in ^ 1u] + (gv >> 5), 1u << (gv & 31u));
+        if (vload(&p.ctl->changed) == 0u) p.ctl->changed = 1u;
+        return;
+    }
     if (p.prefix_scan) {  // flag only; the COMPACT round builds the next frontier
         p.near_stamp[gv] = s.near_epoch;
         L.pushes++;
@@ -914,40 +919,43 @@ __device__ __forceinline__ void async_drain(const RunParams& p, const Snap& s, L
 template <bool ASTAR, int AM>
 __device__ __forceinline__ void round_naive(const RunParams& p, const Snap& s, Local& L) {
     u32* mask_in = p.naive_mask[s.naive_in];
-    u32* mask_out = p.naive_mask[s.naive_in ^ 1u];
-    Ctl* c = p.ctl;
     const u32 stride = gridDim.x * blockDim.x;
     const u32 lane = threadIdx.x & 31u;
-    // Each warp owns aligned groups of 32 vertices = one mask word.
+    // A* bound of this sweep (dist(target) at its start; a stale bound prunes less, never wrongly)
+    u64 ub = ~0ull;
+    if constexpr (ASTAR) ub = astar_bound(p, 0u, 0u);
+    // Each warp owns aligned groups of 32 vertices = one mask word; the arcs of
+    // the word's active vertices are dealt out over the warp's lanes, so a long
+    // row is walked by 32 lanes (two arcs each per step), and a row longer than
+    // 8 CTAs' worth of arcs goes to the grid tier.
     for (u32 v0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; v0 < p.n; v0 += stride) {
         const u32 word = ld_cg(mask_in + (v0 >> 5));
         if (word == 0u) continue;  // warp-uniform
         __syncwarp();
         if (lane == 0) mask_in[v0 >> 5] = 0u;
         const u32 u = v0 + lane;
-        if (!((word >> lane) & 1u) || u >= p.n) continue;
-        const u32 du = st_dist(ld_state(p.state + u));
-        if (du == INF32) continue;
-        u32 ub = INF32;
-        if constexpr (ASTAR) {
-            ub = st_dist(ld_state(p.state + p.target));
-            if ((u64)du + h_of(p, u) >= ub) continue;
-        }
-        const u32 r0 = __ldg(p.prow + u), r1 = __ldg(p.prow + u + 1);
-        for (u32 e = r0; e < r1; ++e) {
-            const uint2 a = __ldg(p.adj + e);
-            if (a.y == PAD_W) break;  // padding is at the end of the row
-            L.edges++;
-            const u64 nd = (u64)du + a.y;
-            if (nd >= INF32) continue;
+        bool act = ((word >> lane) & 1u) && u < p.n;
+        u32 du = INF32, eb = 0, ee = 0;
+        if (act) {
+            du = st_dist(ld_state(p.state + u));
+            act = du != INF32;
             if constexpr (ASTAR) {
-                if (nd + h_of(p, a.x) >= ub) continue;
+                if (act && (u64)du + h_of(p, u) >= ub) act = false;
             }
-            if (relax_state<AM>(p.state + a.x, (u32)nd, u, L.atomics)) {
-                L.updates++;
-                atomicOr(mask_out + (a.x >> 5), 1u << (a.x & 31u));
-                if (vload(&c->changed) == 0u) c->changed = 1u;
-            }
+        }
+        if (act) {
+            eb = __ldg(p.prow + u);
+            ee = __ldg(p.prow + u + 1);
+            if (p.hubs && ee - eb > p.hub_min && hub_publish(p, s, u, eb, ee)) act = false;
+        }
+        relax_items_warp<ASTAR, AM>(p, s, act, u, du, 0u, ub, 0u, eb, ee, L, nullptr);
+    }
+    if (p.hubs) {
+        // every CTA works the sweep's hub records before the barrier
+        __shared__ u32 s_hub[8];
+        if (threadIdx.x == 0) s_hub[0] = 0u;
+        __syncthreads();
+        while (hub_chunk<ASTAR, AM>(p, s, L, nullptr, s_hub)) {
         }
     }
 }

@@ -532,10 +532,12 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
         p.aq = s->d_aq;
     }
 
+    // The naive sweep deals each mask word's arcs over a warp whatever the
+    // mapping; its thread-mapping instantiation measured fastest.
     const int map = mode == MODE_NAIVE ? PFG_MAP_THREAD : o.mapping;
     const int block = o.block_size;
     // Grid tier of the hybrid mapping for rows longer than 8 CTAs' worth of arcs.
-    if (s->d_hubs && map == PFG_MAP_HYBRID && mode != MODE_NAIVE && s->max_deg > 8u * (u32)block) {
+    if (s->d_hubs && (map == PFG_MAP_HYBRID || mode == MODE_NAIVE) && s->max_deg > 8u * (u32)block) {
         p.hubs = s->d_hubs;
         p.hub_cap = s->hub_cap;
         p.hub_min = 8u * (u32)block;
