@@ -178,6 +178,22 @@ PFG_API pfg_status pfg_copy_state(pfg_solver* s, uint64_t first, uint64_t count,
  * so half the bytes cross PCIe. */
 PFG_API pfg_status pfg_copy_dist(pfg_solver* s, uint64_t first, uint64_t count, uint32_t* h_out);
 
+/* Streamed multi-source runs: a sequence of the reference's
+ * GpuSolver::multiSource(srcs, opt, &distOut) calls (src/gpu_sssp.cu:553-569)
+ * in which the copy of one run's distances overlaps the next run's kernel.
+ * pfg_run_dist_async enqueues a run of the k host sources (H2D included) whose
+ * distances go to h_dist_out (k*n words, instance i at i*n; pinned memory makes
+ * the copy asynchronous), after waiting for the previous streamed run's kernel
+ * and starting the copy of that run's distances; prev_stats_out (may be NULL)
+ * receives the previous run's statistics. h_dist_out must stay valid until
+ * pfg_dist_wait returns, which completes the last run and every copy
+ * (stats_out: the last run's statistics). Any other call on the solver first
+ * completes the stream. Errors as pfg_run; a failed run ends the stream. */
+PFG_API pfg_status pfg_run_dist_async(pfg_solver* s, const uint32_t* h_srcs, uint32_t k,
+                                      const pfg_options* opt, uint32_t* h_dist_out,
+                                      pfg_stats* prev_stats_out);
+PFG_API pfg_status pfg_dist_wait(pfg_solver* s, pfg_stats* stats_out);
+
 /* Reconstructs the path src -> dst of instance `inst` of the last run on the
  * device by following parent pointers (reference: reconstructPath,
  * src/cpu_sssp.cpp:124-135). path_len_out = 0 when dst is unreachable or the

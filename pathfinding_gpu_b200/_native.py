@@ -87,6 +87,8 @@ SIGNATURES = {
     "pfg_state_device": (C.c_void_p, [C.c_void_p]),
     "pfg_copy_state": (i32, [C.c_void_p, u64, u64, P(u64)]),
     "pfg_copy_dist": (i32, [C.c_void_p, u64, u64, P(u32)]),
+    "pfg_run_dist_async": (i32, [C.c_void_p, P(u32), u32, C.POINTER(PfgOptions), P(u32), C.POINTER(PfgStats)]),
+    "pfg_dist_wait": (i32, [C.c_void_p, C.POINTER(PfgStats)]),
     "pfg_extract_path": (i32, [C.c_void_p, u32, u32, u32, P(u32), u32, P(u32)]),
     "pfg_query_device": (i32, [i32, P(PfgDeviceInfo)]),
     "pfg_warmup": (i32, []),

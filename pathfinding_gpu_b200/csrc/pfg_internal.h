@@ -90,6 +90,15 @@ struct pfg_solver {
     Ctl* h_ctl = nullptr;       // pinned mirror of the control block
     u32* h_srcs = nullptr;      // pinned staging of the sources [K]
 
+    // streamed multi-source runs (pfg_run_dist_async): the distances of one run
+    // are split into d_dist and copied on copy_stream while the next run computes
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_split = nullptr, ev_copied = nullptr;
+    u32* d_dist = nullptr;        // [K n], allocated on first use
+    uint32_t* pipe_out = nullptr; // host buffer of the streamed run in flight (its copy not started)
+    u32 pipe_k = 0;
+    bool pipe_copying = false;    // a copy may be in flight on copy_stream
+
     // last asynchronous run
     bool pending = false;
     pfg_status pending_status = PFG_OK;

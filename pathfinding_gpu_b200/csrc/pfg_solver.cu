@@ -93,12 +93,16 @@ static void destroy_solver(pfg_solver* s) {
     if (!s) return;
     if (s->device >= 0) cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     for (void* p : s->allocs) cudaFree(p);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->h_srcs) cudaFreeHost(s->h_srcs);
     if (s->d_trace) cudaFree(s->d_trace);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->ev_split) cudaEventDestroy(s->ev_split);
+    if (s->ev_copied) cudaEventDestroy(s->ev_copied);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
     cudaGetLastError();
     delete s;
@@ -616,11 +620,104 @@ static pfg_status complete_run(pfg_solver* s, pfg_stats* stats_out) {
     return PFG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Streamed multi-source runs
+// ---------------------------------------------------------------------------
+// Splits the finished streamed run's distances into d_dist (once the previous
+// copy has drained it) and starts their copy to pipe_out on the copy stream.
+// The run's kernel has completed (complete_run).
+static pfg_status pipe_start_copy(pfg_solver* s) {
+    if (!s->pipe_out) return PFG_OK;
+    const u64 count = (u64)s->pipe_k * s->n;
+    uint32_t* out = s->pipe_out;
+    s->pipe_out = nullptr;
+    PFG_CUDA(cudaStreamWaitEvent(s->stream, s->ev_copied, 0));
+    const cudaError_t e = launch_extract_dist(s->d_state, count, s->d_dist, s->sm_count, s->stream);
+    if (e != cudaSuccess) return fail(PFG_ERR_CUDA, "distance extraction: %s", cudaGetErrorString(e));
+    PFG_CUDA(cudaEventRecord(s->ev_split, s->stream));
+    PFG_CUDA(cudaStreamWaitEvent(s->copy_stream, s->ev_split, 0));
+    PFG_CUDA(cudaMemcpyAsync(out, s->d_dist, count * 4, cudaMemcpyDeviceToHost, s->copy_stream));
+    PFG_CUDA(cudaEventRecord(s->ev_copied, s->copy_stream));
+    s->pipe_copying = true;
+    return PFG_OK;
+}
+
+// Completes a stream of runs: the last run's kernel, its split and copy, and
+// every copy still in flight.
+static pfg_status pipe_flush(pfg_solver* s, pfg_stats* stats_out) {
+    PFG_CUDA(cudaSetDevice(s->device));
+    pfg_status st = PFG_OK;
+    if (s->pipe_out) {
+        st = complete_run(s, stats_out);
+        if (st == PFG_OK) st = pipe_start_copy(s);
+        s->pipe_out = nullptr;
+    }
+    if (s->pipe_copying) {
+        const cudaError_t e = cudaStreamSynchronize(s->copy_stream);
+        s->pipe_copying = false;
+        if (e != cudaSuccess && st == PFG_OK)
+            st = fail(PFG_ERR_CUDA, "distance copy failed: %s", cudaGetErrorString(e));
+    }
+    return st;
+}
+
+// Every other entry point first completes a stream of runs in flight.
+#define PIPE_FLUSH(s)                                          \
+    do {                                                       \
+        if ((s)->pipe_out || (s)->pipe_copying) {              \
+            const pfg_status pst__ = pipe_flush((s), nullptr); \
+            if (pst__ != PFG_OK) return pst__;                 \
+        }                                                      \
+    } while (0)
+
+extern "C" pfg_status pfg_run_dist_async(pfg_solver* s, const uint32_t* h_srcs, uint32_t k,
+                                         const pfg_options* opt, uint32_t* h_dist_out,
+                                         pfg_stats* prev_stats_out) {
+    if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
+    if (!h_srcs || !h_dist_out) return fail(PFG_ERR_INVALID_ARGUMENT, "sources or output are NULL");
+    PFG_CUDA(cudaSetDevice(s->device));
+    if (!s->copy_stream) {
+        PFG_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+        PFG_CUDA(cudaEventCreateWithFlags(&s->ev_split, cudaEventDisableTiming));
+        PFG_CUDA(cudaEventCreateWithFlags(&s->ev_copied, cudaEventDisableTiming));
+    }
+    if (!s->d_dist) {
+        const pfg_status st = s->dalloc(&s->d_dist, (u64)s->K * s->n);
+        if (st != PFG_OK) return st;
+    }
+    if (s->pipe_out) {
+        // the previous streamed run: wait for its kernel, then copy its distances
+        // while the run enqueued below computes
+        pfg_status st = complete_run(s, prev_stats_out);
+        if (st != PFG_OK) {
+            s->pipe_out = nullptr;
+            return st;
+        }
+        st = pipe_start_copy(s);
+        if (st != PFG_OK) return st;
+    } else if (s->pending) {
+        const pfg_status st = complete_run(s, nullptr);
+        (void)st;
+    }
+    const pfg_status st = enqueue_run(s, h_srcs, nullptr, k, 0, 0, opt, true);
+    if (st != PFG_OK) return st;
+    s->pipe_out = h_dist_out;
+    s->pipe_k = k;
+    return PFG_OK;
+}
+
+extern "C" pfg_status pfg_dist_wait(pfg_solver* s, pfg_stats* stats_out) {
+    if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
+    PFG_CUDA(cudaSetDevice(s->device));
+    return pipe_flush(s, stats_out);
+}
+
 extern "C" pfg_status pfg_run(pfg_solver* s, const uint32_t* h_srcs, uint32_t k, int32_t astar,
                               uint32_t dst, const pfg_options* opt, pfg_stats* stats_out,
                               uint64_t* h_state_out, float* ms_out) {
     if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
     if (!h_srcs) return fail(PFG_ERR_INVALID_ARGUMENT, "sources are NULL");
+    PIPE_FLUSH(s);
     if (s->pending) {
         pfg_status st = complete_run(s, nullptr);
         (void)st;
@@ -647,6 +744,7 @@ extern "C" pfg_status pfg_run_traced(pfg_solver* s, const uint32_t* h_srcs, uint
                                      uint32_t trace_cap, uint32_t* rows_out, float* ms_out) {
     if (!s || !h_srcs || !h_trace || !rows_out || trace_cap == 0)
         return fail(PFG_ERR_INVALID_ARGUMENT, "pfg_run_traced: bad argument");
+    PIPE_FLUSH(s);
     PFG_CUDA(cudaSetDevice(s->device));
     if (s->pending) complete_run(s, nullptr);
     if (trace_cap > s->trace_cap) {
@@ -671,6 +769,7 @@ extern "C" pfg_status pfg_run_async(pfg_solver* s, const uint32_t* d_srcs, uint3
                                     int32_t astar, uint32_t dst, const pfg_options* opt) {
     if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
     if (!d_srcs) return fail(PFG_ERR_INVALID_ARGUMENT, "sources are NULL");
+    PIPE_FLUSH(s);
     if (s->pending) {
         pfg_status st = complete_run(s, nullptr);
         (void)st;
@@ -680,11 +779,13 @@ extern "C" pfg_status pfg_run_async(pfg_solver* s, const uint32_t* d_srcs, uint3
 
 extern "C" pfg_status pfg_finish(pfg_solver* s, pfg_stats* stats_out) {
     if (!s) return fail(PFG_ERR_INVALID_ARGUMENT, "solver is NULL");
+    PIPE_FLUSH(s);
     return complete_run(s, stats_out);
 }
 
 extern "C" pfg_status pfg_copy_state(pfg_solver* s, uint64_t first, uint64_t count, uint64_t* h_out) {
     if (!s || !h_out) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
+    PIPE_FLUSH(s);
     if (first + count > (u64)s->K * s->n) return fail(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
     PFG_CUDA(cudaSetDevice(s->device));
     if (s->pending) {
@@ -698,6 +799,7 @@ extern "C" pfg_status pfg_copy_state(pfg_solver* s, uint64_t first, uint64_t cou
 
 extern "C" pfg_status pfg_copy_dist(pfg_solver* s, uint64_t first, uint64_t count, uint32_t* h_out) {
     if (!s || (count > 0 && !h_out)) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
+    PIPE_FLUSH(s);
     if (first + count > (u64)s->K * s->n) return fail(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
     PFG_CUDA(cudaSetDevice(s->device));
     if (s->pending) {
@@ -718,6 +820,7 @@ extern "C" pfg_status pfg_extract_path(pfg_solver* s, uint32_t inst, uint32_t sr
     if (!s || !path_len_out || (cap > 0 && !h_path)) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
     if (inst >= s->K || src >= s->n || dst >= s->n)
         return fail(PFG_ERR_INVALID_ARGUMENT, "instance, source or target out of range");
+    PIPE_FLUSH(s);
     PFG_CUDA(cudaSetDevice(s->device));
     if (s->pending) {
         pfg_status st = complete_run(s, nullptr);
@@ -746,6 +849,7 @@ extern "C" pfg_status pfg_extract_path(pfg_solver* s, uint32_t inst, uint32_t sr
 // Loads a learned-policy network (host PolicyNet image) into the solver.
 extern "C" pfg_status pfg_set_policy(pfg_solver* s, const float* params, uint64_t count) {
     if (!s || !params) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
+    PIPE_FLUSH(s);
     if (count * sizeof(float) != sizeof(PolicyNet))
         return fail(PFG_ERR_INVALID_ARGUMENT, "policy image has %llu floats, expected %llu",
                     (unsigned long long)count, (unsigned long long)(sizeof(PolicyNet) / sizeof(float)));

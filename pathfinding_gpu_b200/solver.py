@@ -251,6 +251,25 @@ class GpuSolver:
             distOut.extend(dist.reshape(k, self.n))
         return r
 
+    def run_dist_async(self, srcs, out: np.ndarray, opt: Optional[GpuOptions] = None) -> GpuStats:
+        """Streamed multiSource: enqueues a run of `srcs` whose distances go to `out`
+        (k*n uint32, pinned for an asynchronous copy; valid until dist_wait) and starts
+        copying the previous streamed run's distances while this one computes.
+        Returns the previous run's statistics."""
+        srcs = np.ascontiguousarray(np.atleast_1d(srcs), np.uint32)
+        assert out.dtype == np.uint32 and out.flags.c_contiguous and out.size >= len(srcs) * self.n
+        c = (opt or GpuOptions()).to_c()
+        st = N.PfgStats()
+        N.check(self._lib.pfg_run_dist_async(self.handle, N.ptr(srcs, N.u32), len(srcs), C.byref(c),
+                                             N.ptr(out, N.u32), C.byref(st)))
+        return GpuStats.from_c(st)
+
+    def dist_wait(self) -> GpuStats:
+        """Completes the stream: the last run and every distance copy."""
+        st = N.PfgStats()
+        N.check(self._lib.pfg_dist_wait(self.handle, C.byref(st)))
+        return GpuStats.from_c(st)
+
     def copy_dist(self, first: int, count: int, out: Optional[np.ndarray] = None) -> np.ndarray:
         """Distances of state words [first, first+count) of the last run (split from
         the packed words on the device; 4 bytes per word cross PCIe)."""

@@ -185,6 +185,26 @@ def test_multisource_dist_out_split_on_device(oracle, grid100, grid100_solver):
         grid100_solver.copy_dist(state.size - 1, 2)
 
 
+def test_streamed_multisource(oracle, grid100, grid100_solver):
+    # runs whose distance copies overlap the next run's kernel: every run's
+    # distances equal the oracle, and a plain run after the stream is unaffected
+    batches = [sources_c0(grid100), [5, 77, 9999], pf.uniform_vertices(grid100.n, 17, 7).tolist(), [1234]]
+    outs = [np.full(len(b) * grid100.n, 7, np.uint32) for b in batches]
+    for b, o in zip(batches, outs):
+        grid100_solver.run_dist_async(b, o, GpuOptions(atomic=AtomicMode.MinNoCheck))
+    grid100_solver.dist_wait()
+    grid100_solver.dist_wait()  # nothing left: a no-op
+    for b, o in zip(batches, outs):
+        for i, s in enumerate(b):
+            assert np.array_equal(o[i * grid100.n:(i + 1) * grid100.n], oracle.sssp_canonical(grid100, s)[0]), (b, i)
+    grid100_solver.run_dist_async([3, 4], outs[1], GpuOptions())
+    check_sssp(oracle, grid100, 42, grid100_solver.sssp(42, GpuOptions()))  # completes the stream first
+    for i, s in enumerate([3, 4]):
+        assert np.array_equal(outs[1][i * grid100.n:(i + 1) * grid100.n], oracle.sssp_canonical(grid100, s)[0])
+    with pytest.raises(pf.PfgError):
+        grid100_solver.run_dist_async(list(range(18)), np.empty(18 * grid100.n, np.uint32))
+
+
 def test_rmat_variants(oracle, rmat12, rmat12_solver):
     srcs = pf.pick_sources(rmat12, 4, SEED)
     for algo, mapping in itertools.product(ALGOS, list(Mapping)):
