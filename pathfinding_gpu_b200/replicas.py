@@ -3,7 +3,8 @@
 A single SSSP does not shard across GPUs at these sizes (it would need an
 all-to-all of remote relaxations on every round), so the multi-GPU form is data
 parallel over independent queries: rank r solves sources r, r+W, r+2W, ... on
-its own GPU and the per-query results are gathered on rank 0. There is no
+its own GPU (serve_sharded: point-to-point queries r, r+W, ... on its own
+serving engine) and the per-query results are gathered on rank 0. There is no
 collective on the data path; the process group only carries barriers, timing
 reductions and the final gather (NCCL on GPUs, gloo on CPU for tests).
 """
@@ -11,7 +12,7 @@ from __future__ import annotations
 
 import os
 from datetime import timedelta
-from typing import Callable, List, Optional, Sequence
+from typing import Callable, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -92,6 +93,17 @@ class ReplicaGroup:
         if self.dist:
             self.dist.destroy_process_group()
             self.dist = None
+
+
+def serve_sharded(pairs: Sequence[Tuple[int, int]], group: ReplicaGroup,
+                  answer: Callable[[List[Tuple[int, int]]], Sequence[int]]) -> Optional[np.ndarray]:
+    """Point-to-point queries sharded round-robin over the replicas: each rank
+    answers its shard with `answer` (pairs -> target distances; on a GPU, its own
+    GpuServer through serving.answer_all) and rank 0 gathers the distances in
+    query order (None on the other ranks)."""
+    mine = shard(list(pairs), group.rank, group.world)
+    d = np.asarray(answer(mine) if mine else [], np.uint32).reshape(-1, 1)
+    return group.gather_rows(d, len(pairs))
 
 
 def solve_sharded(sources: Sequence[int], group: ReplicaGroup,

@@ -112,6 +112,13 @@ class GpuServer:
         return out + self.results()
 
 
+def answer_all(server: GpuServer, pairs: Sequence[Tuple[int, int]], max_rounds: int = 8) -> List[int]:
+    """Target distances of `pairs` (in order), all admitted at once and drained."""
+    ids = [server.submit(int(s), int(t)) for s, t in pairs]
+    got = {r["id"]: r["dist"] for r in server.drain(max_rounds=max_rounds)}
+    return [got[q] for q in ids]
+
+
 def run_poisson(server: GpuServer, pairs: Sequence[Tuple[int, int]], rate_qps: float, max_rounds: int = 32,
                 seed: int = 0, time_limit_s: float = 120.0) -> Dict:
     """Real-time replay of Poisson arrivals at `rate_qps`; latency = finish - scheduled arrival."""

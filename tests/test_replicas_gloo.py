@@ -1,6 +1,7 @@
 """Replica sharding over a 2-rank gloo process group on CPU (the N > 1 path of bench.py
 and pathfinding_gpu_b200.replicas): each rank solves its round-robin shard of the
-sources with the oracle and rank 0 must gather exactly the single-process answer."""
+sources (solve_sharded) and of point-to-point queries (serve_sharded) with the oracle,
+and rank 0 must gather exactly the single-process answer."""
 import os
 import socket
 import sys
@@ -23,7 +24,7 @@ def _worker(rank, world, port, out_path):
     os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
                       MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import pathfinding_gpu_b200 as pf
-    from pathfinding_gpu_b200.replicas import ReplicaGroup, solve_sharded, shard
+    from pathfinding_gpu_b200.replicas import ReplicaGroup, serve_sharded, solve_sharded, shard
     from oracle import oracle as O
 
     g = pf.grid(40, 40, 2026)
@@ -35,11 +36,13 @@ def _worker(rank, world, port, out_path):
         return np.stack([O.dijkstra(g, s)[0] for s in mine])
 
     got = solve_sharded(srcs, group, solve)
+    pairs = [(int(a), int(b)) for a, b in pf.uniform_vertices(g.n, 2 * 5, 123).reshape(-1, 2)]
+    got_pairs = serve_sharded(pairs, group, lambda mine: [int(O.dijkstra(g, s)[0][t]) for s, t in mine])
     mx = group.max(float(rank + 1))
     sm = group.sum(float(rank + 1))
     group.barrier()
     if rank == 0:
-        np.savez(out_path, got=got, mx=mx, sm=sm)
+        np.savez(out_path, got=got, mx=mx, sm=sm, got_pairs=got_pairs)
     group.close()
 
 
@@ -68,3 +71,6 @@ def test_two_rank_gloo_replicas(tmp_path):
     res = np.load(out)
     assert np.array_equal(res["got"], want)
     assert float(res["mx"]) == 2.0 and float(res["sm"]) == 3.0
+    pairs = [(int(a), int(b)) for a, b in pf.uniform_vertices(g.n, 2 * 5, 123).reshape(-1, 2)]
+    want_pairs = np.array([[O.dijkstra(g, s)[0][t]] for s, t in pairs], np.uint32)
+    assert np.array_equal(res["got_pairs"], want_pairs)

@@ -72,3 +72,13 @@ def test_poisson_stream_latencies(oracle, road):
     got = {r["id"] - 1: r["dist"] for r in rep["results"]}
     assert got == want
     assert 0 < rep["p50_ms"] <= rep["p99_ms"]
+
+
+def test_answer_all_in_query_order(oracle, road):
+    # the per-replica answer function of serve_sharded: distances in query order
+    from pathfinding_gpu_b200.serving import answer_all
+    v = pf.uniform_vertices(road.n, 2 * 12, 77)
+    pairs = [(int(v[2 * i]), int(v[2 * i + 1])) for i in range(12)]
+    with GpuServer(road, slots=5) as srv:
+        got = answer_all(srv, pairs)
+    assert got == [int(oracle.dijkstra(road, s)[0][t]) for s, t in pairs]
