@@ -61,7 +61,7 @@ def HEADLINE_OPTIONS():
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=BATCH)
@@ -89,13 +89,14 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host time of arrival, csv line)
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
@@ -105,7 +106,14 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def start_window(self):
+        self.window = [time.perf_counter(), None]
+
+    def end_window(self):
+        if self.window:
+            self.window[1] = time.perf_counter()
 
     def __exit__(self, *exc):
         if self.proc:
@@ -118,7 +126,12 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines
+        if self.window and self.window[1] is not None:
+            # samples that arrived while the timed region ran (lines come a few ms late)
+            inside = [x for x in lines if self.window[0] <= x[0] <= self.window[1] + 0.03]
+            lines = inside or lines[-1:]
+        for _, ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -236,6 +249,7 @@ def run_ours(args, D):
            for _ in range(args.steps)]
     launches = 0
     with ClockSampler(D.local) as clk:
+        clk.start_window()
         for i in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.zero_()  # L2 flush between timed steps (256 MB > 126 MB L2)
@@ -245,6 +259,7 @@ def run_ours(args, D):
             evs[i][1].record(stream)
             finish()
         torch.cuda.synchronize()
+        clk.end_window()
     D.barrier()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     local_total = sum(step_ms)
