@@ -332,6 +332,7 @@ static pfg_status batch_prepare(pfg_batch* b, const pfg_options* opt_in, RunPara
     p.adj = b->d_adj;
     p.prow = b->d_prow;
     p.row_stride = b->row_stride;
+    p.short_rows = b->max_deg <= 32u ? 1u : 0u;
     p.n = (u32)std::min<u64>(b->total_states, 0xFFFFFFFFull);
     p.maxw = b->maxw;
     p.avg_w = b->avg_w;

@@ -225,6 +225,7 @@ struct RunParams {
     // (no row has more arcs): row u of a graph starts at prow[first row] +
     // ROW_ALIGN * u, so an item's arcs are addressed without loading prow.
     u32 row_stride;
+    u32 short_rows;    // 1 when no row has more than 32 arcs: the CTA-cooperative path is never needed
     u32* aq;           // ring counters, see RingCounter
     int test_absent_cta;  // test hook: CTA 0 leaves at once, so every barrier wait runs out
     HubRec* hubs;      // hub records (nullptr: no row of the graph is long enough)

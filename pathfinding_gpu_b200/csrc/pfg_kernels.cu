@@ -550,7 +550,8 @@ __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, b
         }
     } else {
         // short rows only: each warp balances its own items; else the CTA does
-        if (__syncthreads_or(act && ee - eb > WARP_ROW_MAX))
+        // (no CTA vote when no row of the graph has more than 32 arcs)
+        if (!p.short_rows && __syncthreads_or(act && ee - eb > WARP_ROW_MAX))
             relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
         else
             relax_items_warp<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cl);
@@ -737,8 +738,8 @@ __device__ __forceinline__ void async_drain(const RunParams& p, const Snap& s, L
         s_idle = 0u;
         s_hub[0] = 0u;
     }
+    __syncthreads();  // (each pass ends with a barrier after its pushes)
     for (;;) {
-        __syncthreads();
         if (threadIdx.x == 0) {
             // appends past cl_head + CL_CAP went to the ring already
             u32 tail = cs.cl_n;

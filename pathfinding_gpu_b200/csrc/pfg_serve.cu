@@ -391,6 +391,7 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
     p.adj = s->d_adj;
     p.prow = s->d_prow;
     p.row_stride = s->row_stride;
+    p.short_rows = s->max_deg <= 32u ? 1u : 0u;
     p.x = s->d_x;
     p.y = s->d_y;
     p.n = n;

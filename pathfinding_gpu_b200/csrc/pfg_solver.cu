@@ -486,6 +486,7 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     p.adj = s->d_adj;
     p.prow = s->d_prow;
     p.row_stride = s->row_stride;
+    p.short_rows = s->max_deg <= 32u ? 1u : 0u;
     p.x = s->d_x;
     p.y = s->d_y;
     p.n = s->n;
