@@ -80,3 +80,13 @@ def test_cpp_dropin_header_is_self_contained(tmp_path):
     r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", f"-I{ROOT/'include'}", f"-I{compat}", str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_streamed_and_copy_entry_points_reject_null_before_touching_a_gpu():
+    # argument checks of the distance copy-back and streamed multiSource entry points
+    lib = N.load()
+    st = N.PfgStats()
+    assert lib.pfg_dist_wait(None, C.byref(st)) == 1
+    assert b"NULL" in lib.pfg_last_error()
+    assert lib.pfg_run_dist_async(None, None, 1, None, None, None) == 1
+    assert lib.pfg_copy_dist(None, 0, 1, None) == 1
