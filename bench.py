@@ -375,6 +375,40 @@ def cpu_baseline(g, srcs, sample: int):
             "sample": f"{len(srcs)} of the step's sources, cpuMultiSource OpenMP x{threads}"}
 
 
+def _opt_dict(o):
+    from dataclasses import asdict
+    return {k: (v.name if hasattr(v, "name") else v) for k, v in asdict(o).items()}
+
+
+def cpu_single_thread(g, gr, src, pairs):
+    """cpuDijkstra (1 thread) on the 1000x1000 grid and R-MAT-20 and cpuAStar on a sample of
+    the grid's 256 pairs, from the reference's own code (oracle/_ref) when built, else the
+    oracle's restatement."""
+    from oracle import oracle as O
+    use_ref = O.ref_available()
+    out = {"cores": 1, "kind": "reference" if use_ref else "port"}
+    for name, graph, srcs in (("grid1000", g, [src] + pf_sources(g, 2)), ("rmat20", gr, pf_sources(gr, 3))):
+        R = O.RefGraph.wrap(graph) if use_ref else None
+        ms = []
+        for s_ in srcs:
+            ms.append(R.dijkstra(int(s_))[3] if use_ref else O.dijkstra(graph, int(s_))[3])
+        deg = np.diff(graph.row_offsets).astype(np.int64)
+        out[f"{name}_cpuDijkstra_ms"] = round(statistics.median(ms), 2)
+        out[f"{name}_cpuDijkstra_sources"] = len(srcs)
+    R = O.RefGraph.wrap(g) if use_ref else None
+    ams = []
+    for a, b in pairs[:64]:
+        ams.append(R.astar(int(a), int(b))[3] if use_ref else O.astar(g, int(a), int(b))[3])
+    out["grid1000_cpuAStar_ms"] = {"mean": round(float(np.mean(ams)), 3), "pairs": len(ams),
+                                   "sample": "the first 64 of the 256 pairs"}
+    return out
+
+
+def pf_sources(graph, k):
+    import pathfinding_gpu_b200 as pf
+    return pf.pick_sources(graph, k, 99).tolist()
+
+
 def _median_ms(fn, reps=5):
     fn()
     return statistics.median(fn() for _ in range(reps))
@@ -387,20 +421,46 @@ def extras(g):
     out = {}
     t0 = time.perf_counter()
     # --- the 1000x1000 grid: single-source modes and 256 A* pairs ---
+    pairs = pf.uniform_vertices(g.n, 2 * 256, SEED + 7).reshape(-1, 2)
+    src = int(pf.uniform_vertices(g.n, 1, SEED)[0])
     with pf.GpuSolver(g, 1) as s:
-        src = int(pf.uniform_vertices(g.n, 1, SEED)[0])
         for algo in (GpuAlgo.DeltaStep, GpuAlgo.Frontier, GpuAlgo.NaiveRelax):
             o = GpuOptions(algo=algo)
             out[f"grid1000_sssp_{algo.name}_ms"] = round(_median_ms(lambda: s.run_state([src], o, copy=False)[1], 3), 3)
-        pairs = pf.uniform_vertices(g.n, 2 * 256, SEED + 7).reshape(-1, 2)
         ts = [s.run_state([int(a)], GpuOptions(), astar=True, dst=int(b), copy=False)[1] for a, b in pairs]
         out["grid1000_astar_256_pairs_ms"] = {"mean": round(float(np.mean(ts)), 3),
                                               "p50": round(float(np.percentile(ts, 50)), 3),
                                               "p99": round(float(np.percentile(ts, 99)), 3)}
-    # --- R-MAT scale 20: learned policy vs fixed automatic Delta (same engine, same sources) ---
+    # --- aggregate throughput against the batch size (roofline per launch) ---
+    peak, _ = measured_peaks()
+    sweep = {}
+    Ks = (16, 32, 64, 128, 256)
+    srcs_all = pf.uniform_vertices(g.n, max(Ks), SEED)
+    with pf.GpuSolver(g, max(Ks)) as s:
+        for K in Ks:
+            o = HEADLINE_OPTIONS()
+            ms = _median_ms(lambda: s.run_state(srcs_all[:K], o, copy=False)[1], 3)
+            b_alg = K * (16.0 * g.m + 20.0 * g.n)  # grid: every arc and vertex reachable
+            sweep[str(K)] = {"ms": round(ms, 3), "gteps": round(K * g.m / ms / 1e6, 3),
+                             "roofline_frac": round(b_alg / (ms * 1e-3) / 1e9 / peak, 4)}
+    out["grid1000_batch_sweep"] = sweep
+    # --- R-MAT scale 20: batched multi-source throughput, learned policy vs fixed automatic Delta ---
     from pathfinding_gpu_b200 import policy as P
+    gr = pf.rmat(20, 16, seed=SEED)
+    deg = np.diff(gr.row_offsets).astype(np.int64)
+    rsrcs = pf.pick_sources(gr, 16, SEED)
+    with pf.GpuSolver(gr, 16) as s:
+        o = HEADLINE_OPTIONS()
+        _, _, state = s.run_state(rsrcs, o)
+        dist = pf.unpack(state)[0].reshape(16, gr.n)
+        reach = dist != 0xFFFFFFFF
+        m_r = int((deg[None, :] * reach).sum())
+        n_r = int(reach.sum())
+        ms = _median_ms(lambda: s.run_state(rsrcs, o, copy=False)[1], 3)
+        out["rmat20_batch16"] = {"ms": round(ms, 3), "gteps": round(m_r / ms / 1e6, 3),
+                                 "roofline_frac": round((16.0 * m_r + 20.0 * n_r) / (ms * 1e-3) / 1e9 / peak, 4),
+                                 "reachable_arcs": m_r}
     if P.WEIGHTS.exists():
-        gr = pf.rmat(20, 16, seed=SEED)
         with pf.GpuSolver(gr, 1) as s:
             s.set_policy(P.load())
             rows = []
@@ -417,8 +477,12 @@ def extras(g):
                              "work_per_m_learned": round(st_l.edgesScanned / gr.m, 3)})
             out["rmat20_learned_vs_fixed"] = {"median_speedup": statistics.median(r["speedup"] for r in rows),
                                               "runs": rows}
-    # --- uneven batch in one launch, replayed from a CUDA graph ---
+    # --- the reference's own CPU code, single thread, on the same inputs ---
+    out["cpu_reference_single_thread"] = cpu_single_thread(g, gr, src, pairs)
+    # --- uneven batch in one launch, schedule from the autotuner, replayed from a CUDA graph ---
     from pathfinding_gpu_b200.batch import GpuBatch
+    from pathfinding_gpu_b200 import autotune
+    import tempfile
     big = pf.grid(1024, 1024, SEED)
     small = pf.grid_batch(256, 32, 316, SEED)
     graphs = [big] + small
@@ -427,12 +491,20 @@ def extras(g):
     states = 64 * big.n + sum(gs.n for gs in small)
     with GpuBatch(graphs, max_states=states, max_instances=len(inst)) as b:
         b.set_instances(inst)
-        o = GpuOptions(atomic=pf.AtomicMode.MinNoCheck)
-        run_ms = _median_ms(lambda: b.run(o)[1], 3)
-        b.capture(o)
+        o_default = GpuOptions(atomic=pf.AtomicMode.MinNoCheck)
+        default_ms = _median_ms(lambda: b.run(o_default)[1], 3)
+        os.environ.setdefault("PFG_TUNE_CACHE", str(Path(tempfile.gettempdir()) / "pfg_bench_tune.json"))
+        key = f"batch-{len(graphs)}graphs-{len(inst)}inst-{states}states-{big.n}big"
+        auto_delta = b.run(o_default)[0].delta
+        tuned, tuned_ms, log = autotune.tune(lambda o: b.run(o)[1], o_default, auto_delta, reps=2,
+                                             key=key, use_cache=False)
+        run_ms = _median_ms(lambda: b.run(tuned)[1], 3)
+        b.capture(tuned)
         rep_ms = _median_ms(lambda: b.replay()[1], 5)
         arcs = 64 * big.m + sum(gs.m for gs in small)
         out["batch_uneven"] = {"instances": len(inst), "states": states, "arcs": arcs,
+                               "default_options_ms": round(default_ms, 3),
+                               "tuned_key": key, "tuned_options": _opt_dict(tuned), "tuner_trials": len(log),
                                "run_ms": round(run_ms, 3), "replay_ms": round(rep_ms, 3),
                                "gteps_replay": round(arcs / rep_ms / 1e6, 3)}
     # --- A* serving with continuous batching on the 2048x2048 road-like graph ---
@@ -452,56 +524,61 @@ def extras(g):
     return out
 
 
-def run_reference(args, D):
-    if D.rank != 0:
+def run_reference(args):
+    """The reference's own cpuMultiSource (OpenMP, every host thread) on the step's full
+    batch: the graph is built from the benchmark grid's arcs by the reference's own
+    buildCSR, and the sources are the step's; nothing of this repository's engine is
+    loaded. Under torchrun only rank 0 runs."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return None
-    import pathfinding_gpu_b200 as pf
     from oracle import oracle as O
-    g, srcs = workload(0, args.batch)
     K = args.batch
+    n, s, d, w, x, y = O.config_grid_arcs(GRID_SIDE, GRID_SIDE, SEED)
+    srcs = O.uniform_vertices(n, K, SEED)
     if O.ref_available():
-        R = O.RefGraph.wrap(g)
-        run = lambda s: R.multi_source(s, 0, False)
+        R = O.ref_build_csr(n, s, d, w, x, y)
+        run = lambda ss: R.multi_source(ss, 0, False)
         threads = O.ref().ref_max_threads()
         kind = "reference"
+        m = R.arrays()[5]["m"]
     else:
-        run = lambda s: O.multi_source(g, s, 0, False)
+        g = O.config_grid(GRID_SIDE, GRID_SIDE, SEED)
+        run = lambda ss: O.multi_source(g, ss, 0, False)
         threads = O.max_threads()
         kind = "port"
-    sample = min(K, max(threads, 8))
-    sub = np.asarray(srcs[:sample], np.uint32)
+        m = g.m
     for _ in range(args.warmup):
-        run(sub[: max(1, threads)])
+        run(srcs[: max(1, threads)])
     times = []
     for _ in range(args.steps):
-        ms, _, _ = run(sub)
+        ms, _, _ = run(srcs)
         times.append(ms)
     ms_step = statistics.mean(times)
-    m_r = g.m * sample
+    m_r = m * K  # the grid is strongly connected: every arc is reachable from every source
     value = m_r / (ms_step * 1e-3) / 1e9
     return {
         "impl": "reference",
         "metric": "GTEPS (reachable arcs / s, SSSP Delta-stepping, batch of sources)",
-        "value": round(value, 4), "unit": "GTEPS", "n_gpus": D.world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+        "value": round(value, 4), "unit": "GTEPS", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": f"grid{GRID_SIDE}x{GRID_SIDE} multiSource K={K} Delta-stepping",
-                   "n": g.n, "m": g.m, "batch": K, "cpu_sources_per_step": sample},
+                   "n": n, "m": m, "batch": K, "cpu_sources_per_step": K},
         "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": int(threads), "kind": kind,
-                         "sample": f"{sample} sources per step, cpuMultiSource OpenMP x{threads}"},
+                         "sample": f"all {K} sources of the step, cpuMultiSource OpenMP x{threads}"},
         "e2e": {"value": round(value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
 def main():
     args = parse()
+    if args.impl == "reference":
+        res = run_reference(args)
+        if res is not None:
+            print(json.dumps(res))
+        return
     D = Dist(args.gpus)
     try:
-        if args.impl == "reference":
-            res = run_reference(args, D)
-            if D.rank == 0 and res is not None:
-                print(json.dumps(res))
-            return
         res, g, srcs = run_ours(args, D)
         if D.rank == 0:
             if D.world == 1:

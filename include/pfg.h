@@ -291,12 +291,14 @@ PFG_API double pfg_server_now_us(const pfg_server* v);
 PFG_API pfg_solver* pfg_server_solver(pfg_server* v);
 
 /* ---- learned Delta policy (extension; no reference counterpart) ----
- * The policy is a 12 -> 64 -> 64 -> 64 -> 8 fp32 MLP evaluated on the device
- * at every bucket advance; its argmax picks the next bucket's Delta as one of
- * {1/4, 1/2, 1, 2, 4, 8, 16, 64} x the automatic Delta. It only changes the
- * schedule: distances and parents are the same as with a fixed Delta.
+ * The policy is a 12 -> 64 -> 64 -> 64 -> 16 fp32 MLP evaluated on the device
+ * at the first bucket and at every bucket advance; its argmax class c picks
+ * the next bucket's Delta as {1/16, 1/8, 1/4, 1/2, 1, 2, 4, 8}[c % 8] x the
+ * automatic Delta and its schedule (asynchronous bucket if c < 8, relaxation
+ * rounds otherwise). It only changes the schedule: distances and parents are
+ * the same as with a fixed Delta.
  * pfg_set_policy loads a flat parameter image of pfg_policy_param_count()
- * floats (layout: w1[64x12] b1 w2[64x64] b2 w3[64x64] b3 w4[8x64] b4
+ * floats (layout: w1[64x12] b1 w2[64x64] b2 w3[64x64] b3 w4[16x64] b4
  * in_mean[12] in_scale[12]). */
 PFG_API pfg_status pfg_set_policy(pfg_solver* s, const float* params, uint64_t count);
 PFG_API uint64_t pfg_policy_param_count(void);
@@ -309,7 +311,7 @@ PFG_API pfg_status pfg_run_traced(pfg_solver* s, const uint32_t* h_srcs, uint32_
                                   uint32_t trace_cap, uint32_t* rows_out, float* ms_out);
 /* Training and inference of the policy network on the GPU (hand-written
  * kernels). Samples are rows of 12 features (h_x, n x 12) with soft targets
- * over the 8 Delta classes (h_y, n x 8, each row summing to 1); the loss is
+ * over the 16 classes (h_y, n x 16, each row summing to 1); the loss is
  * the mean cross-entropy. pfg_policy_grad returns the loss and its gradient
  * for every parameter (zero for the fixed input normalisation);
  * pfg_policy_train runs `steps` full-batch Adam steps in place and writes the
@@ -329,12 +331,24 @@ PFG_API pfg_status pfg_policy_infer(const float* h_params, const float* h_x, uin
  * may use, or a latency-critical loop that cannot afford cudaMalloc's
  * implicit synchronisation. Runs the persistent Delta-stepping kernel of
  * pfg_run (Hybrid mapping, MinRBA atomics, fixed `delta` >= 1) from `src`
- * on a CSR already in device memory (rows sorted by weight, weights >= 1),
- * writing n packed (dist << 32 | parent) words to d_state_out and
- * [status, rounds, buckets, non-empty rounds] to d_status_out[0..3]
- * (status is a pfg_status value). Work is enqueued on `stream` (a
- * cudaStream_t of the current device) and the call returns without waiting;
- * read d_status_out after synchronising.
+ * on a CSR already in device memory, writing n packed (dist << 32 | parent)
+ * words to d_state_out and [status, rounds, buckets, non-empty rounds] to
+ * d_status_out[0..3] (status is a pfg_status value). Work is enqueued on
+ * `stream` (a cudaStream_t of the current device) and the call returns
+ * without waiting; read d_status_out after synchronising.
+ * The CSR must be what pfg_create accepts: row_offsets[0] = 0, non-decreasing,
+ * row_offsets[n] = m, col < n, weights in [1, 2^32 - 2], every row sorted by
+ * weight. The host cannot read device memory without waiting, so these are
+ * checked on the device: when one fails, nothing is relaxed, d_state_out is
+ * (PFG_INF, PFG_NO_PARENT) everywhere, d_status_out[0] is
+ * PFG_ERR_INVALID_GRAPH (PFG_ERR_CAPACITY when the rows padded to 4 arcs do
+ * not fit the scratch), d_status_out[1] the mask of failed checks (1 row
+ * offsets, 2 padded size, 4 column, 8 weight, 16 row order) and [2], [3] zero.
+ * Differences from pfg_run: buckets always run as relaxation rounds (no
+ * asynchronous buckets: they need a ring sized by the graph), rows of any
+ * length are relaxed by the CTA that holds them (no hub records), and eager
+ * sub-rounds follow pfg_run's default (on when m / n <= 6). Every device-side
+ * wait is bounded by PFG_TIMEOUT_MS, as in pfg_run. Results are identical.
  * All scratch lives in one fixed device array compiled into the library
  * (about 7.6 MB, held by every device the library's module is loaded on
  * until the process exits), so the graph is limited to n <=

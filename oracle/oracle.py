@@ -124,6 +124,55 @@ def gen_grid_road(rows, cols, seed):
     return n, s[:m].copy(), d[:m].copy(), w[:m].copy(), x, y
 
 
+class ArcGraph:
+    """A plain CSR (row_offsets, col_indices, weights, x, y, hScale) for the oracle's callers."""
+
+    def __init__(self, row, col, w, x, y, stats):
+        self.row_offsets, self.col_indices, self.weights = row, col, w
+        self.x, self.y = x, y
+        self.n, self.m = len(row) - 1, len(col)
+        self.hScale = stats["hScale"]
+        self.stats = stats
+
+
+def config_grid_arcs(rows, cols, seed):
+    """Arc list of the benchmark grid: vertex (r, c) at coordinates (x = c, y = r), arcs
+    both ways to the right and lower neighbours, each direction with its own weight
+    llround(100 * U[1, 1.5)) drawn from the reference's SplitMix64 stream in
+    row-major vertex order (right pair first, then the lower pair)."""
+    r, c = np.divmod(np.arange(rows * cols, dtype=np.int64), cols)
+    ids = r * cols + c
+    right, down = c + 1 < cols, r + 1 < rows
+    cnt = 2 * right.astype(np.int64) + 2 * down.astype(np.int64)
+    m = int(cnt.sum())
+    start = np.concatenate([[0], np.cumsum(cnt)[:-1]])
+    src = np.empty(m, np.int64)
+    dst = np.empty(m, np.int64)
+    i = start[right]
+    src[i], dst[i] = ids[right], ids[right] + 1
+    src[i + 1], dst[i + 1] = ids[right] + 1, ids[right]
+    j = start[down] + 2 * right[down]
+    src[j], dst[j] = ids[down], ids[down] + cols
+    src[j + 1], dst[j + 1] = ids[down] + cols, ids[down]
+    z = rng_stream(seed, m)
+    u = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    w = np.floor(100.0 * (1.0 + 0.5 * u) + 0.5)  # llround of a positive value
+    x, y = c.astype(np.float64), r.astype(np.float64)
+    return rows * cols, src.astype(np.uint32), dst.astype(np.uint32), w.astype(np.uint32), x, y
+
+
+def config_grid(rows, cols, seed) -> ArcGraph:
+    """The benchmark grid built by the oracle's buildCSR restatement."""
+    n, s, d, w, x, y = config_grid_arcs(rows, cols, seed)
+    row, col, wt, stats = build_csr(n, s, d, w, x, y)
+    return ArcGraph(row, col, wt, x, y, stats)
+
+
+def uniform_vertices(n, count, seed) -> np.ndarray:
+    """`count` vertices uniform in [0, n): successive SplitMix64 outputs modulo n."""
+    return (rng_stream(seed, count) % np.uint64(n)).astype(np.uint32)
+
+
 def gen_rmat_ref(scale, ef, maxw, seed):
     n = 1 << scale
     cap = 2 * n * ef + 8
@@ -258,6 +307,14 @@ def ref() -> C.CDLL:
         R.ref_pick_sources.argtypes = [C.c_void_p, u32, u64, P(u32)]
         R.ref_heuristic.restype = u32
         R.ref_heuristic.argtypes = [f64, f64, f64, f64, f64]
+        R.ref_load_dimacs.restype = C.c_void_p
+        R.ref_load_dimacs.argtypes = [C.c_char_p, C.c_char_p]
+        R.ref_load_snap.restype = C.c_void_p
+        R.ref_load_snap.argtypes = [C.c_char_p, i32, u32, u64]
+        R.ref_load_binary.restype = C.c_void_p
+        R.ref_load_binary.argtypes = [C.c_char_p]
+        R.ref_save_binary.restype = i32
+        R.ref_save_binary.argtypes = [C.c_void_p, C.c_char_p]
         _ref = R
     return _ref
 
@@ -327,6 +384,29 @@ class RefGraph:
         out = np.empty(count, np.uint32)
         ref().ref_pick_sources(self.h, count, seed, _p(out, u32))
         return out
+
+    def save_binary(self, path) -> bool:
+        """The reference's saveBinary (PFCSR001 cache file)."""
+        return ref().ref_save_binary(self.h, str(path).encode()) == 1
+
+
+def _loaded(h) -> Optional[RefGraph]:
+    return RefGraph(h) if h else None
+
+
+def ref_load_dimacs(gr, co=None) -> Optional[RefGraph]:
+    """The reference's loadDIMACS + buildCSR; None when its loader fails."""
+    return _loaded(ref().ref_load_dimacs(str(gr).encode(), None if co is None else str(co).encode()))
+
+
+def ref_load_snap(path, symmetrize=True, max_w=1000, seed=2026) -> Optional[RefGraph]:
+    """The reference's loadSNAP + buildCSR; None when its loader fails."""
+    return _loaded(ref().ref_load_snap(str(path).encode(), 1 if symmetrize else 0, max_w, seed))
+
+
+def ref_load_binary(path) -> Optional[RefGraph]:
+    """The reference's loadBinary (PFCSR001); None when its loader fails."""
+    return _loaded(ref().ref_load_binary(str(path).encode()))
 
 
 def ref_gen_grid_road(rows, cols, seed) -> RefGraph:

@@ -124,6 +124,29 @@ void ref_pick_sources(void* h, u32 count, u64 seed, u32* out) {
     std::copy(s.begin(), s.end(), out);
 }
 
+// The reference's loaders (graph.cpp: loadDIMACS, loadSNAP, loadBinary,
+// saveBinary); a loaded edge list goes through buildCSR as in its main.cpp.
+// NULL (or 0) when the reference's loader reports failure.
+void* ref_load_dimacs(const char* gr, const char* co) {
+    EdgeList el;
+    if (!loadDIMACS(gr, co ? co : "", el)) return nullptr;
+    return wrap(buildCSR(std::move(el)));
+}
+
+void* ref_load_snap(const char* path, int symmetrize, u32 maxw, u64 seed) {
+    EdgeList el;
+    if (!loadSNAP(path, symmetrize != 0, maxw, seed, el)) return nullptr;
+    return wrap(buildCSR(std::move(el)));
+}
+
+void* ref_load_binary(const char* path) {
+    CSRGraph g;
+    if (!loadBinary(path, g)) return nullptr;
+    return wrap(std::move(g));
+}
+
+int ref_save_binary(void* h, const char* path) { return saveBinary(((RefGraph*)h)->g, path) ? 1 : 0; }
+
 u32 ref_heuristic(double xv, double yv, double xt, double yt, double scale) {
     return heuristicValue(xv, yv, xt, yt, scale);
 }

@@ -16,7 +16,7 @@ from dataclasses import asdict, replace
 from pathlib import Path
 from typing import Callable, Dict, Optional, Tuple
 
-from .solver import AtomicMode, GpuAlgo, GpuOptions, Mapping
+from .solver import AtomicMode, Compaction, GpuAlgo, GpuOptions, Mapping, Policy, Schedule
 
 LAUNCH_SHAPES = [(256, 4), (512, 2), (1024, 1)]       # (threads per CTA, CTAs per SM)
 ATOMICS = [AtomicMode.MinRBA, AtomicMode.MinNoCheck]
@@ -64,7 +64,8 @@ def cached(key: str) -> Optional[GpuOptions]:
     o = e["options"]
     return GpuOptions(algo=GpuAlgo(o["algo"]), mapping=Mapping(o["mapping"]), atomic=AtomicMode(o["atomic"]),
                       delta=o["delta"], blockSize=o["blockSize"], syncEvery=o["syncEvery"],
-                      eager=o["eager"], blocksPerSM=o["blocksPerSM"])
+                      compaction=Compaction(o.get("compaction", 0)), policy=Policy(o.get("policy", 0)),
+                      eager=o["eager"], blocksPerSM=o["blocksPerSM"], schedule=Schedule(o.get("schedule", 0)))
 
 
 def tune(time_fn: Callable[[GpuOptions], float], base: GpuOptions, auto_delta: int, reps: int = 2,

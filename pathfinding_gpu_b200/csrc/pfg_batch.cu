@@ -498,7 +498,8 @@ extern "C" uint64_t pfg_batch_device_bytes(const pfg_batch* b) { return b ? b->b
 
 extern "C" pfg_status pfg_batch_copy_state(pfg_batch* b, uint64_t first, uint64_t count, uint64_t* h_out) {
     if (!b || !h_out) return set_error(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (first + count > b->total_states) return set_error(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
+    if (first > b->total_states || count > b->total_states - first)  // (no sum that can wrap)
+        return set_error(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
     B_CUDA(cudaSetDevice(b->device));
     B_CUDA(cudaMemcpyAsync(h_out, b->d_state + first, count * 8, cudaMemcpyDeviceToHost, b->stream));
     B_CUDA(cudaStreamSynchronize(b->stream));

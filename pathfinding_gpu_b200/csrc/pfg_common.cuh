@@ -77,7 +77,7 @@ enum RunMode : int { MODE_NAIVE = 0, MODE_FRONTIER = 1, MODE_DELTA = 2 };
 enum CounterSlot : u32 { C_NEAR0 = 0, C_NEAR1 = 1, C_FAR0 = 2, C_FAR1 = 3, C_R = 4, C_COUNT = 8 };
 
 // Device status words (match pfg_status values).
-enum DevStatus : u32 { DS_OK = 0, DS_BAD_SOURCE = 1, DS_NOT_CONVERGED = 4, DS_TIMEOUT = 5 };
+enum DevStatus : u32 { DS_OK = 0, DS_BAD_SOURCE = 1, DS_BAD_GRAPH = 2, DS_NOT_CONVERGED = 4, DS_TIMEOUT = 5 };
 
 // Which device-side wait ran out of time (Ctl::wait_site; outside the words a
 // transition stores back, so a concurrent transition never erases it).

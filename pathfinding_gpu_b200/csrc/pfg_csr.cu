@@ -361,7 +361,7 @@ extern "C" pfg_status pfg_csr_build_device(uint32_t n, uint64_t m_in, const uint
     C_CUDA(cudaMemcpyAsync(&h_kept, kept, 8, cudaMemcpyDeviceToHost, st));
     C_CUDA(cudaStreamSynchronize(st));
     if (h_flags[0]) return set_error(PFG_ERR_INVALID_GRAPH, "arc endpoint out of range");
-    if (h_kept >= 0xFFFFFFFFull) return set_error(PFG_ERR_INVALID_GRAPH, "Graph too large: m must be < 2^32");
+    if (h_kept >= 0xFFFFFFFFull) return set_error(PFG_ERR_INVALID_GRAPH, "%llu arcs remain after dropping self loops; at most 2^32 - 2 fit the 32-bit row offsets", (unsigned long long)h_kept);
     const u32 m = (u32)h_kept;
 
     k_scan_blocks<<<nb, SCAN_B, 0, st>>>(deg, n, d_row, bsum);

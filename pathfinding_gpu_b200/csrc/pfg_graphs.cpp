@@ -89,7 +89,9 @@ pfg_status build_csr(u32 n, const std::vector<u32>& src, const std::vector<u32>&
             keep++;
         }
     }
-    if (keep >= 0xFFFFFFFFull) return gfail(PFG_ERR_INVALID_GRAPH, "Graph too large: m must be < 2^32");
+    if (keep >= 0xFFFFFFFFull)
+        return gfail(PFG_ERR_INVALID_GRAPH, std::to_string(keep) +
+                                                " arcs remain after dropping self loops; at most 2^32 - 2 fit the 32-bit row offsets");
     pfg_graph* g = new pfg_graph();
     g->n = n;
     g->m = (u32)keep;

@@ -29,6 +29,12 @@ void sanitize_options(pfg_options& o);
 // Launch shape: CTAs per SM for the persistent kernel.
 int blocks_per_sm_for(const pfg_options& o, bool astar, int map);
 
+// Eager sub-rounds per grid round of the hybrid mapping when the caller leaves
+// the choice to the engine (pfg_options::eager < 0), and the average degree
+// above which the engine turns them off (hubs make in-round propagation redundant).
+constexpr int kDefaultEager = 4;
+constexpr double kEagerMaxAvgDegree = 6.0;
+
 // Eager sub-rounds when the caller leaves the choice to the engine.
 u32 eager_rounds_for(const pfg_options& o);
 

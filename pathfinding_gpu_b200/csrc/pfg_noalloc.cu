@@ -17,6 +17,7 @@
 // process exits. Graphs larger than the limits below are rejected.
 #include "../../include/pfg.h"
 #include "pfg_common.cuh"
+#include "pfg_internal.h"
 #include "pfg_kernels.h"
 
 #include <cuda_runtime.h>
@@ -59,40 +60,100 @@ pfg_status na_fail(pfg_status st, const char* msg) {
     return st;
 }
 
-// Padded row starts (rows rounded up to 4 arcs) and their total, by one CTA.
-__global__ void k_na_pad_rows(const u32* __restrict__ row, u32 n, u32* __restrict__ prow) {
-    __shared__ u32 part[1024];
+// Failed device-side checks of the caller's CSR (bits of the error word in
+// the scratch, reported in d_status_out[1]).
+constexpr u32 kBadRows = 1u;       // row_offsets[0] != 0, row_offsets[n] != m, or a decreasing offset
+constexpr u32 kBadCapacity = 2u;   // the rows padded to 4 arcs do not fit the scratch
+constexpr u32 kBadColumn = 4u;     // col_indices[k] >= n
+constexpr u32 kBadWeight = 8u;     // weights[k] == 0 or 2^32 - 1
+constexpr u32 kBadOrder = 16u;     // a row is not sorted by weight
+
+// Checks the row offsets and writes the padded row starts (rows rounded up to
+// 4 arcs), by one CTA of 1024 threads. Nothing is written to prow when a check
+// fails: the error word is set and the later kernels of the call leave the
+// scratch alone, so a malformed CSR cannot make any kernel of this call write
+// outside the scratch or the caller's output.
+__global__ void k_na_pad_rows(const u32* __restrict__ row, u32 n, u32 m, u32* __restrict__ prow,
+                              u32* __restrict__ err) {
+    __shared__ unsigned long long part[1024];
+    __shared__ u32 s_bad;
     const u32 t = threadIdx.x, T = blockDim.x;
+    if (t == 0) s_bad = 0u;
+    __syncthreads();
     const u32 per = (n + T - 1) / T;
     const u32 b = min(n, t * per), e = min(n, b + per);
-    u32 sum = 0;
-    for (u32 u = b; u < e; ++u) sum += (row[u + 1] - row[u] + ROW_ALIGN - 1) / ROW_ALIGN * ROW_ALIGN;
+    unsigned long long sum = 0;
+    u32 bad = 0;
+    for (u32 u = b; u < e; ++u) {
+        const u32 r0 = row[u], r1 = row[u + 1];
+        if (r1 < r0) bad |= kBadRows;
+        else sum += (r1 - r0 + ROW_ALIGN - 1) / ROW_ALIGN * ROW_ALIGN;
+    }
+    if (t == 0 && (row[0] != 0u || row[n] != m)) bad |= kBadRows;
+    if (bad) atomicOr(&s_bad, bad);
     part[t] = sum;
     __syncthreads();
     if (t == 0) {  // n <= 65536: a serial pass over T partial sums is cheap
-        u32 acc = 0;
+        unsigned long long acc = 0;
         for (u32 i = 0; i < T; ++i) {
-            const u32 v = part[i];
+            const unsigned long long v = part[i];
             part[i] = acc;
             acc += v;
         }
-        prow[n] = acc;
+        if (acc > kMaxPaddedArcs) s_bad |= kBadCapacity;
+        *err = s_bad;
+        if (!s_bad) prow[n] = (u32)acc;
     }
     __syncthreads();
-    u32 acc = part[t];
+    if (s_bad) return;  // block-uniform
+    u32 acc = (u32)part[t];
     for (u32 u = b; u < e; ++u) {
         prow[u] = acc;
         acc += (row[u + 1] - row[u] + ROW_ALIGN - 1) / ROW_ALIGN * ROW_ALIGN;
     }
 }
 
+// One warp per vertex copies its row into the padded slot, checking every arc:
+// a column >= n or a weight outside [1, 2^32 - 2] is replaced by a padding arc
+// (so the relaxation could never leave the state array) and, like a row that
+// is not sorted by weight, sets the error word, which cancels the run. Does
+// nothing when the row offsets failed their checks.
+__global__ void k_na_build_adj(const u32* __restrict__ row, const u32* __restrict__ col,
+                               const u32* __restrict__ w, const u32* __restrict__ prow, u32 n,
+                               uint2* __restrict__ adj, u32* __restrict__ err) {
+    if (*(volatile u32*)err) return;  // written by k_na_pad_rows, earlier on the same stream
+    const u32 lane = threadIdx.x & 31u;
+    const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
+    u32 bad = 0;
+    for (u32 u = warp; u < n; u += nwarps) {
+        const u32 r0 = row[u], deg = row[u + 1] - r0;
+        const u32 p0 = prow[u], pd = prow[u + 1] - p0;  // pd >= deg: rows were checked
+        for (u32 j = lane; j < pd; j += 32) {
+            uint2 a = make_uint2(u, PAD_W);
+            if (j < deg) {
+                const u32 c = col[r0 + j], ww = w[r0 + j];
+                if (c >= n) bad |= kBadColumn;
+                else if (ww == 0u || ww == PAD_W) bad |= kBadWeight;
+                else a = make_uint2(c, ww);
+                if (j > 0 && w[r0 + j - 1] > ww) bad |= kBadOrder;
+            }
+            adj[p0 + j] = a;
+        }
+    }
+    if (bad) atomicOr(err, bad);
+}
+
 // Control block of one run; the persistent epoch counters restart at 0 because
 // the stamp words were just cleared.
-__global__ void k_na_init(Ctl* ctl, u32* src_slot, u32 src, u32 delta, u32 round_cap) {
+// A failed CSR check (error word != 0) starts the run with a bad-graph status:
+// the persistent kernel then only initialises the output and stops.
+__global__ void k_na_init(Ctl* ctl, u32* src_slot, const u32* err, u32 src, u32 delta, u32 round_cap) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     Ctl c;
     memset(&c, 0, sizeof(c));
     c.rd.phase = PH_INIT;
+    c.rd.status = *err ? (u32)DS_BAD_GRAPH : (u32)DS_OK;
     c.rd.delta = delta;
     c.rd.heavy = 1u;  // the largest weight is not known here; the light/heavy split handles any Delta
     c.rd.map_mode = 1u;
@@ -104,9 +165,19 @@ __global__ void k_na_init(Ctl* ctl, u32* src_slot, u32 src, u32 delta, u32 round
 }
 
 // Copies the outcome of the run into the caller's status words:
-// [0] pfg_status of the run, [1] device rounds, [2] buckets, [3] non-empty rounds.
-__global__ void k_na_status(const Ctl* ctl, u32* out) {
+// [0] pfg_status of the run, [1] device rounds, [2] buckets, [3] non-empty rounds;
+// for a graph that failed the device-side checks [0] is PFG_ERR_INVALID_GRAPH
+// (PFG_ERR_CAPACITY when its padded rows do not fit the scratch), [1] the mask
+// of failed checks and [2], [3] zero.
+__global__ void k_na_status(const Ctl* ctl, const u32* err, u32* out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const u32 bad = *err;
+    if (bad) {
+        out[0] = (bad & kBadCapacity) ? (u32)PFG_ERR_CAPACITY : (u32)PFG_ERR_INVALID_GRAPH;
+        out[1] = bad;
+        out[2] = out[3] = 0u;
+        return;
+    }
     const u32 ds = ctl->rd.status;
     out[0] = ds == DS_OK ? (u32)PFG_OK
            : ds == DS_BAD_SOURCE ? (u32)PFG_ERR_INVALID_ARGUMENT
@@ -188,6 +259,7 @@ extern "C" pfg_status pfg_sssp_noalloc(const uint32_t* d_row_offsets, const uint
 
     Ctl* ctl = (Ctl*)(base + kOffCtl);
     u32* src_slot = (u32*)(base + kOffSrc);
+    u32* err = src_slot + 1;  // failed CSR checks of this call (bits kBad*)
     u32* prow = (u32*)(base + kOffProw);
     uint2* adj = (uint2*)(base + kOffAdj);
     u32* q = (u32*)(base + kOffQueues);
@@ -196,13 +268,17 @@ extern "C" pfg_status pfg_sssp_noalloc(const uint32_t* d_row_offsets, const uint
     // The stamp words must start at zero (their epochs restart with the control block).
     cudaError_t e = cudaMemsetAsync(stamps, 0, 3 * (size_t)n * 4, s);
     if (e == cudaSuccess) {
-        k_na_pad_rows<<<1, 1024, 0, s>>>(d_row_offsets, n, prow);
+        k_na_pad_rows<<<1, 1024, 0, s>>>(d_row_offsets, n, m, prow, err);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = launch_build_adj(d_row_offsets, d_col_indices, d_weights, prow, n, adj, s);
+    if (e == cudaSuccess) {
+        const u32 blocks = std::max<u32>(1u, std::min<u32>((n + 7u) / 8u, 4096u));
+        k_na_build_adj<<<blocks, 256, 0, s>>>(d_row_offsets, d_col_indices, d_weights, prow, n, adj, err);
+        e = cudaGetLastError();
+    }
     const u32 round_cap = (u32)std::min<unsigned long long>(4ull * n + 1000ull, 0x7FFFFFFFull);
     if (e == cudaSuccess) {
-        k_na_init<<<1, 1, 0, s>>>(ctl, src_slot, src, delta, round_cap);
+        k_na_init<<<1, 1, 0, s>>>(ctl, src_slot, err, src, delta, round_cap);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
@@ -228,14 +304,16 @@ extern "C" pfg_status pfg_sssp_noalloc(const uint32_t* d_row_offsets, const uint
         p.ctl = ctl;
         p.delta = delta;
         p.mode = MODE_DELTA;
-        p.eager = 4;
+        // the engine defaults of pfg_run: eager sub-rounds on low-degree graphs
+        // only, the PFG_TIMEOUT_MS bound on every device-side wait
+        p.eager = (double)m / (double)n > kEagerMaxAvgDegree ? 0u : kDefaultEager;
         const int grid = g_dev_sms[dev] * g_dev_bps[dev];
         p.eager_max_items = (u32)std::max(1, grid * 1024 / 4);
-        p.timeout_ns = 2000000000ull;
+        p.timeout_ns = device_timeout_ns();
         e = launch_persistent(p, false, PFG_ATOMIC_MIN_RBA, PFG_MAP_HYBRID, 1024, grid, s);
     }
     if (e == cudaSuccess) {
-        k_na_status<<<1, 1, 0, s>>>(ctl, d_status_out);
+        k_na_status<<<1, 1, 0, s>>>(ctl, err, d_status_out);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {

@@ -367,11 +367,6 @@ static int env_int(const char* name, int dflt) {
     return atoi(v);
 }
 
-// Eager sub-rounds per grid round of the hybrid mapping when the caller leaves
-// the choice to the engine (pfg_options::eager < 0).
-static const int kDefaultEager = 4;
-static const double kEagerMaxAvgDegree = 6.0;
-
 namespace pfg {
 
 pfg_options default_options() {
@@ -787,7 +782,10 @@ extern "C" pfg_status pfg_finish(pfg_solver* s, pfg_stats* stats_out) {
 extern "C" pfg_status pfg_copy_state(pfg_solver* s, uint64_t first, uint64_t count, uint64_t* h_out) {
     if (!s || !h_out) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
     PIPE_FLUSH(s);
-    if (first + count > (u64)s->K * s->n) return fail(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
+    // (written so that no sum can wrap around 2^64)
+    const u64 total_states = (u64)s->K * s->n;
+    if (first > total_states || count > total_states - first)
+        return fail(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
     PFG_CUDA(cudaSetDevice(s->device));
     if (s->pending) {
         pfg_status st = complete_run(s, nullptr);
@@ -801,7 +799,10 @@ extern "C" pfg_status pfg_copy_state(pfg_solver* s, uint64_t first, uint64_t cou
 extern "C" pfg_status pfg_copy_dist(pfg_solver* s, uint64_t first, uint64_t count, uint32_t* h_out) {
     if (!s || (count > 0 && !h_out)) return fail(PFG_ERR_INVALID_ARGUMENT, "NULL argument");
     PIPE_FLUSH(s);
-    if (first + count > (u64)s->K * s->n) return fail(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
+    // (written so that no sum can wrap around 2^64)
+    const u64 total_states = (u64)s->K * s->n;
+    if (first > total_states || count > total_states - first)
+        return fail(PFG_ERR_INVALID_ARGUMENT, "range outside the state");
     PFG_CUDA(cudaSetDevice(s->device));
     if (s->pending) {
         pfg_status st = complete_run(s, nullptr);

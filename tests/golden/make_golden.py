@@ -13,6 +13,7 @@ itself is not available.
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 from pathlib import Path
 
@@ -28,7 +29,8 @@ SEED = 2026
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("PFG_REFERENCE", str(ROOT.parent / "reference")),
+                    help="reference checkout (default: $PFG_REFERENCE, else ../reference beside the repository)")
     args = ap.parse_args()
     O.build(args.reference)
     if not O.ref_available():

@@ -48,3 +48,23 @@ def test_astar_to_itself_and_duplicate_sources(oracle):
         d_ref, p_can = oracle.sssp_canonical(g, src)
         assert np.array_equal(d[i * g.n:(i + 1) * g.n], d_ref)
         assert np.array_equal(p[i * g.n:(i + 1) * g.n], p_can)
+
+
+def test_copy_ranges_that_would_wrap_are_rejected():
+    # first + count past 2^64 must not pass the range check (the kernel would read
+    # before the state array); both copy entry points refuse without touching the device
+    import ctypes as C
+    from pathfinding_gpu_b200 import _native as N
+    g = pf.grid(10, 10, 1)
+    with pf.GpuSolver(g, 2) as s:
+        s.sssp(0, GpuOptions())
+        lib = s._lib
+        out32 = np.zeros(4, np.uint32)
+        out64 = np.zeros(4, np.uint64)
+        huge = (1 << 64) - 1
+        assert lib.pfg_copy_dist(s.handle, huge, 2, N.ptr(out32, N.u32)) == 1
+        assert lib.pfg_copy_state(s.handle, huge, 2, N.ptr(out64, N.u64)) == 1
+        assert lib.pfg_copy_dist(s.handle, 2 * g.n - 1, 2, N.ptr(out32, N.u32)) == 1
+        assert lib.pfg_copy_dist(s.handle, 2 * g.n - 2, 2, N.ptr(out32, N.u32)) == 0
+        assert lib.pfg_copy_state(s.handle, huge, 2, N.ptr(out64, N.u64)) == 1
+        assert b"range outside the state" in lib.pfg_last_error()

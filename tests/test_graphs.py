@@ -132,3 +132,16 @@ def test_snap_loader(tmp_path):
     w01 = g.weights[np.flatnonzero(g.col_indices[g.row_offsets[0]:g.row_offsets[1]] == 1)[0]]
     w10 = g.weights[g.row_offsets[1] + np.flatnonzero(g.col_indices[g.row_offsets[1]:g.row_offsets[2]] == 0)[0]]
     assert w01 == w10 and 1 <= w01 <= 1000
+
+
+def test_oracle_restates_the_benchmark_grid():
+    # the oracle's generator of the benchmark grid (used by bench.py's reference arm,
+    # which must not load this library) builds the same CSR as pfg_graph_gen_grid
+    from oracle import oracle as O
+    for rows, cols, seed in ((100, 100, 2026), (37, 53, 5), (1000, 1000, 2026)):
+        a = O.config_grid(rows, cols, seed)
+        g = pf.grid(rows, cols, seed)
+        assert np.array_equal(a.row_offsets, g.row_offsets) and np.array_equal(a.col_indices, g.col_indices)
+        assert np.array_equal(a.weights, g.weights) and np.array_equal(a.x, g.x) and np.array_equal(a.y, g.y)
+        assert a.hScale == g.hScale and a.stats["avgW"] == g.avgW
+    assert np.array_equal(O.uniform_vertices(10 ** 6, 64, 2026), pf.uniform_vertices(10 ** 6, 64, 2026))
