@@ -82,7 +82,7 @@ enum DevStatus : u32 { DS_OK = 0, DS_BAD_SOURCE = 1, DS_BAD_GRAPH = 2, DS_NOT_CO
 // Which device-side wait ran out of time (Ctl::wait_site; outside the words a
 // transition stores back, so a concurrent transition never erases it).
 enum WaitSite : u32 { WS_NONE = 0, WS_RING_PUSH = 1, WS_DRAIN_IDLE = 2, WS_SPILL_SLOT = 3, WS_RING_SLOT = 4,
-                      WS_BARRIER = 5 };
+                      WS_BARRIER = 5, WS_LOCAL_SLOT = 6 };
 inline const char* wait_site_name(u32 w) {
     switch (w) {
         case WS_RING_PUSH: return "a ring-queue push waiting for a free slot";
@@ -90,6 +90,7 @@ inline const char* wait_site_name(u32 w) {
         case WS_SPILL_SLOT: return "a claimed-list spill waiting for a free ring slot";
         case WS_RING_SLOT: return "a ring-queue pop waiting for its item to be written";
         case WS_BARRIER: return "the grid barrier";
+        case WS_LOCAL_SLOT: return "a CTA work-queue slot hand-over";
     }
     return "a device-side wait";
 }
@@ -232,6 +233,16 @@ struct RunParams {
     u32 hub_cap;       // records available
     u32 hub_min;       // items with more selected arcs are published as hubs
     u32 hub_chunk;     // arcs per claimed chunk
+    // Asynchronous drains by warp workers (warp_drain = 1): every warp of a CTA
+    // takes entries from the CTA's shared-memory work queue on its own, with no
+    // block barrier between batches; rows above hub_min_warp selected arcs are
+    // worked in chunks by all warps of the CTA (and rows above hub_min by any
+    // CTA through hub records, claimed hub_chunk_warp arcs at a time).
+    // warp_drain = 0: the CTA works its claimed list in block-synchronous passes.
+    u32 warp_drain;
+    u32 hub_min_warp;
+    u32 hub_chunk_warp;
+    u32 pad_wd;
 };
 
 // ---------------------------------------------------------------------------

@@ -24,6 +24,7 @@
 #include "pfg_kernels.h"
 
 #include <atomic>
+#include <cstddef>
 #include <cstdio>
 
 namespace pfg {
@@ -44,10 +45,26 @@ typedef Rd Snap;
 struct Local {
     u32 edges = 0, atomics = 0, updates = 0, pushes = 0;
     u32 edges_flushed = 0;  // value of `edges` at the last per-round flush (policy / trace)
+    u32 spilled = 0;   // warp drain: this thread pushed to the ring since its warp's last batch ended
     u64 fmin = ~0ull;  // smallest key this thread pushed to the far pile this round
 };
 
 constexpr u32 CL_CAP = 2048;  // claimed-list entries per CTA (hybrid mapping)
+
+// A row task of the warp drain. claim packs (generation:16 | len:24 | next:24):
+// a chunk is claimed by a compare-and-swap that advances `next` while next < len,
+// and a task cannot complete (and its slot be reused) while a claimed chunk is
+// unfinished, so the fields read after a successful claim are the task's.
+constexpr u32 TASK_CAP = 8;
+struct __align__(16) RowTask {
+    unsigned long long claim;
+    unsigned long long ub;  // A* pruning bound of the item
+    u32 gi, u, du, ib, inst, eb, len;
+    u32 done;   // arcs relaxed; the chunk that completes the row closes the task
+    u32 free;   // 1: the slot may take a new task
+    u32 pad[3];
+};
+static_assert(sizeof(RowTask) == 64, "RowTask layout");
 
 // Per-CTA shared memory of the hybrid mapping (dynamic shared memory). The
 // edge-balanced mapping's per-thread arrays follow the struct, sized by the
@@ -61,8 +78,41 @@ struct Coop {
     u32 cl_head;     // first position not yet taken (rounds: always 0; asynchronous buckets: advances)
     u32 cl_base;
     u32 pad;
+    // Asynchronous drain by warp workers: cl and cl_d together hold the CTA's
+    // work queue, CL_CAP 64-bit slots of (queued distance << 32 | state index),
+    // RING_FREE when free. Positions are reserved with shared-memory atomics;
+    // a slot is handed over by its contents (a pusher waits for RING_FREE, a
+    // popper for an entry), so any warp pushes and any warp pops.
+    u32 wq_head;     // positions reserved by poppers
+    u32 wq_tail;     // positions reserved by pushers
+    u32 wq_pending;  // work the CTA holds (see warp_drain); > 0 exactly while it holds a busy unit
+    u32 wq_agent;    // 1 while one warp polls the ring / hub records / termination for the CTA
+    u32 wq_exit;     // 1: the bucket is drained (or the run failed): every warp leaves
+    u32 wq_idle;     // 1 while the CTA is counted in the ring's idle counter
+    u32 wq_hint;     // idle CTAs last seen by this CTA: > 0 makes producers spill to the ring
+    u32 wq_beats;    // batches relaxed by this CTA and global progress seen by its agent (wait limits)
+    u32 wq_backoff;  // idle poll interval (ns), doubled while the agent finds nothing
+    u32 hub_cursor;  // first hub record of the drain this CTA has not passed
+    u32 wq_beat_seen;  // last value of the ring's heartbeat seen by the CTA's agent
+    u32 task_open;   // row tasks posted and not yet complete
+    u32 pad2[4];
+    // Ring positions [lo, hi) the CTA's agent took from the ring (hi << 32 | lo);
+    // any warp of the CTA pops batches from it.
+    unsigned long long rr;
+    unsigned long long pad3;
+    // Row tasks: rows of more than RunParams::hub_min_warp selected arcs that a
+    // warp met in its batch, worked in chunks by every warp of the CTA.
+    RowTask task[TASK_CAP];
 };
 static_assert(sizeof(Coop) % 16 == 0, "the per-thread arrays after Coop need 16-byte alignment");
+static_assert(offsetof(Coop, cl) % 8 == 0 && offsetof(Coop, cl_d) == offsetof(Coop, cl) + 4 * CL_CAP,
+              "cl and cl_d form the 64-bit work-queue slots of the warp drain");
+static_assert(offsetof(Coop, rr) % 8 == 0 && offsetof(Coop, task) % 16 == 0, "Coop alignment");
+constexpr u32 WQ_CAP = CL_CAP;
+constexpr u32 WQ_MASK = WQ_CAP - 1u;
+__device__ __forceinline__ unsigned long long* wq_slots(Coop& cs) {
+    return reinterpret_cast<unsigned long long*>(cs.cl);
+}
 
 // Bytes of dynamic shared memory for a CTA of `block` threads: Coop, then
 // u64 ub[block], u32 off[block + 1], eb[block], u[block], du[block], ib[block], inst[block].
@@ -154,6 +204,73 @@ __device__ __forceinline__ u32 light_end(const uint2* adj, u32 r0, u32 r1, u32 d
 }
 
 // ---------------------------------------------------------------------------
+// Work queue of the warp drain (shared memory; any warp pushes, any warp pops)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u32 vld_s(const u32* q) { return *(const volatile u32*)q; }
+
+// Entries one warp takes at a time (one per lane).
+constexpr u32 WQ_BATCH = 32;
+
+// Reserves cnt push positions [base, base + cnt); false when the queue lacks
+// room (or the reservation keeps losing races): the caller uses the ring.
+__device__ __forceinline__ bool wq_reserve(Coop& cs, u32 cnt, u32& base) {
+    u32 t = vld_s(&cs.wq_tail);
+    for (int tries = 0; tries < 64; ++tries) {
+        const u32 used = t - vld_s(&cs.wq_head);
+        if ((int)used >= 0 && used + cnt > WQ_CAP) return false;
+        const u32 o = atomicCAS(&cs.wq_tail, t, t + cnt);
+        if (o == t) {
+            base = t;
+            return true;
+        }
+        t = o;
+    }
+    return false;
+}
+
+// Writes the entry of reserved position pos once the slot's previous entry has
+// been taken (bounded wait; on timeout the run fails).
+__device__ __forceinline__ void wq_write(Coop& cs, u32 pos, unsigned long long ent, const RunParams& p) {
+    unsigned long long* slot = wq_slots(cs) + (pos & WQ_MASK);
+    if (atomicCAS(slot, RING_FREE, ent) == RING_FREE) return;
+    const u64 t0 = global_timer_ns();
+    while (atomicCAS(slot, RING_FREE, ent) != RING_FREE) {
+        if (global_timer_ns() - t0 > p.timeout_ns) {
+            flag_timeout(p.ctl, WS_LOCAL_SLOT);
+            return;
+        }
+        __nanosleep(20);
+    }
+}
+
+// Warp-aggregated push of one entry per calling lane into the CTA's queue,
+// counted as pending work first (the pushing warp holds pending work itself,
+// so the count never reaches zero early). False for the whole group when the
+// queue is full, or when other CTAs are idle and this CTA already keeps one
+// entry per thread (a batch for each of its warps): the entries then go to
+// the ring, where idle CTAs take them.
+__device__ __forceinline__ bool wq_push(Coop& cs, unsigned long long ent, const RunParams& p) {
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    const u32 cnt = __popc(mask);
+    u32 base = 0, ok = 0;
+    if (lane == leader) {
+        const u32 backlog = vld_s(&cs.wq_tail) - vld_s(&cs.wq_head);
+        if (!(vld_s(&cs.wq_hint) > 0u && (int)backlog > (int)blockDim.x)) {
+            atomicAdd(&cs.wq_pending, cnt);
+            ok = wq_reserve(cs, cnt, base) ? 1u : 0u;
+            if (!ok) atomicSub(&cs.wq_pending, cnt);
+        }
+    }
+    ok = __shfl_sync(mask, ok, leader);
+    if (!ok) return false;
+    base = __shfl_sync(mask, base, leader);
+    wq_write(cs, base + __popc(mask & ((1u << lane) - 1u)), ent, p);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // Relaxation of one arc (u -> v, w) and queueing of the improved head.
 // ---------------------------------------------------------------------------
 // cl != nullptr (hybrid mapping): a claimed near vertex goes to the CTA's
@@ -170,6 +287,14 @@ __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, 
     if (!near) {
         queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gv);
         if (p.inst_far_cnt) atomicAdd(p.inst_far_cnt + inst, 1u);
+        return;
+    }
+    if (s.async_bkt && p.warp_drain) {
+        // asynchronous bucket drained by warp workers: the CTA's work queue, else the ring
+        const unsigned long long ent = ((unsigned long long)nd << 32) | gv;
+        if (cl && wq_push(*cl, ent, p)) return;
+        L.spilled = 1u;
+        if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, ent, p.timeout_ns)) flag_timeout(c, WS_RING_PUSH);
         return;
     }
     if (cl) {
@@ -286,13 +411,82 @@ __device__ __forceinline__ void relax_arc_pair(const RunParams& p, const Snap& s
 // (two arcs per load; rows start on 32-byte boundaries).
 template <bool ASTAR, int AM>
 __device__ __forceinline__ void relax_range_thread(const RunParams& p, const Snap& s, u32 u, u32 du,
-                                                   u32 ib, u64 ub, u32 inst, u32 eb, u32 ee, Local& L) {
+                                                   u32 ib, u64 ub, u32 inst, u32 eb, u32 ee, Local& L,
+                                                   Coop* cl = nullptr) {
     const uint4* a4 = reinterpret_cast<const uint4*>(p.adj);
     for (u32 e = eb & ~1u; e < ee; e += 2) {
         const uint4 q = __ldg(a4 + (e >> 1));
-        if (e >= eb) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, inst, q.x, q.y, L, nullptr);
-        if (e + 1 < ee) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, inst, q.z, q.w, L, nullptr);
+        if (e >= eb) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, inst, q.x, q.y, L, cl);
+        if (e + 1 < ee) relax_arc<ASTAR, AM>(p, s, u, du, ib, ub, inst, q.z, q.w, L, cl);
     }
+}
+
+// State updates of up to four arcs (u -> hv[j], hw[j]) of one lane, all issued
+// before any result is used (one dependent round of L2 round trips). Only the
+// 32-bit candidate distances stay live across the round; A* keys of the
+// improved heads are recomputed (cheap next to the relaxations).
+template <bool ASTAR, int AM>
+__device__ __forceinline__ void relax4(const RunParams& p, const Snap& s, u32 u, u32 du, u32 ib, u64 ub, u32 inst,
+                                       const u32 (&hv)[4], const u32 (&hw)[4], Local& L, Coop* cl) {
+    u32 nd[4];
+    bool go[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        u64 d = 0, k = 0;
+        go[j] = arc_candidate<ASTAR>(p, du, ub, inst, hv[j], hw[j], L, d, k);
+        nd[j] = (u32)d;
+    }
+    if constexpr (AM == 1) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) go[j] = go[j] && relax_state<1>(p.state + ib + hv[j], nd[j], u, L.atomics);
+    } else {
+        if constexpr (AM == 0) {  // read before atomic: all reads in flight, then the atomics
+            u64 cur[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) cur[j] = go[j] ? ld_state(p.state + ib + hv[j]) : 0ull;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) go[j] = go[j] && cur[j] > pack_state(nd[j], u);
+        }
+        unsigned long long old[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            old[j] = go[j] ? atomicMin((unsigned long long*)(p.state + ib + hv[j]),
+                                       (unsigned long long)pack_state(nd[j], u))
+                           : ~0ull;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            L.atomics += go[j] ? 1u : 0u;
+            go[j] = go[j] && st_dist(old[j]) > nd[j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (go[j]) {
+            u64 key = nd[j];
+            if constexpr (ASTAR) key = astar_key(p, inst, hv[j], nd[j]);
+            after_improve(p, s, ib + hv[j], key, nd[j], inst, L, cl);
+        }
+    }
+}
+
+// Fixed 4-slot rows (every row of the graph has at most 4 arcs): the lane that
+// holds an item loads its whole row, one 32-byte sector, with two 128-bit loads
+// and updates all its arcs in one round (relax4). eb is the row start; [eb, ee)
+// the selected arcs (ee <= eb + 4).
+template <bool ASTAR, int AM>
+__device__ __forceinline__ void relax_quad(const RunParams& p, const Snap& s, bool act, u32 u, u32 du, u32 ib,
+                                           u64 ub, u32 inst, u32 eb, u32 ee, Local& L, Coop* cl) {
+    uint4 q0 = make_uint4(0u, PAD_W, 0u, PAD_W), q1 = q0;
+    if (act) {
+        const uint4* a4 = reinterpret_cast<const uint4*>(p.adj + eb);
+        q0 = __ldg(a4);
+        q1 = __ldg(a4 + 1);
+    }
+    const u32 cnt = act ? ee - eb : 0u;
+    const u32 hv[4] = {q0.x, q0.z, q1.x, q1.z};
+    const u32 hw[4] = {cnt > 0u ? q0.y : PAD_W, cnt > 1u ? q0.w : PAD_W, cnt > 2u ? q1.y : PAD_W,
+                       cnt > 3u ? q1.w : PAD_W};
+    relax4<ASTAR, AM>(p, s, u, du, ib, ub, inst, hv, hw, L, cl);
 }
 
 // Instance, state base, row base and local vertex of state index gi.
@@ -532,7 +726,7 @@ __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, b
                                             u32 ib, u64 ub, u32 inst, u32 eb, u32 ee, Local& L, Coop& cs,
                                             Coop* cl, int kind) {
     if constexpr (MAP == 0) {  // thread per item
-        if (act) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, inst, eb, ee, L);
+        if (act) relax_range_thread<ASTAR, AM>(p, s, u, du, ib, ub, inst, eb, ee, L, cl);
     } else if constexpr (MAP == 1) {  // warp per item
         const u32 lane = threadIdx.x & 31u;
         unsigned ballot = __ballot_sync(FULL, act);
@@ -545,7 +739,7 @@ __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, b
             const u32 web = __shfl_sync(FULL, eb, leader), wee = __shfl_sync(FULL, ee, leader);
             for (u32 e = web + lane; e < wee; e += 32) {
                 const uint2 a = __ldg(p.adj + e);
-                relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, winst, a.x, a.y, L, nullptr);
+                relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, winst, a.x, a.y, L, cl);
             }
         }
     } else {
@@ -558,17 +752,18 @@ __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, b
     }
 }
 
-// Publishes the hub row [eb, ee) of item gi; false if the record table is
-// full (the caller then relaxes the row itself). In an asynchronous drain
-// (phase ASYNC) the record holds a busy unit until its last chunk is relaxed;
-// in a round every CTA works the round's records before the barrier.
-__device__ __forceinline__ bool hub_publish(const RunParams& p, const Snap& s, u32 gi, u32 eb, u32 ee) {
+// Publishes the hub row [eb, ee) of item gi and returns its record index, or
+// ~0u if the record table is full (the caller then relaxes the row itself). In
+// an asynchronous drain (phase ASYNC) the record holds a busy unit until its
+// last chunk is relaxed; in a round every CTA works the round's records before
+// the barrier.
+__device__ __forceinline__ u32 hub_publish_at(const RunParams& p, const Snap& s, u32 gi, u32 eb, u32 ee) {
     const bool drain = s.phase == PH_ASYNC;
     if (drain) atomicAdd(p.aq + AQ_BUSY, 1u);
     const u32 k = atomicAdd(p.aq + AQ_HUBS, 1u);
     if (k >= p.hub_cap) {
         if (drain) atomicSub(p.aq + AQ_BUSY, 1u);
-        return false;
+        return ~0u;
     }
     HubRec* r = p.hubs + k;
     r->gi = gi;
@@ -578,7 +773,12 @@ __device__ __forceinline__ bool hub_publish(const RunParams& p, const Snap& s, u
     r->done = 0u;
     __threadfence();
     atomicExch(&r->ready, s.near_epoch);
-    return true;
+    return k;
+}
+
+// Publishes a hub record (see hub_publish_at); false if the table is full.
+__device__ __forceinline__ bool hub_publish(const RunParams& p, const Snap& s, u32 gi, u32 eb, u32 ee) {
+    return hub_publish_at(p, s, gi, eb, ee) != ~0u;
 }
 
 // Claims the next chunk of a published hub row (records from the CTA's cursor
@@ -911,6 +1111,486 @@ __device__ __forceinline__ void async_drain(const RunParams& p, const Snap& s, L
         cs.cl_n = 0u;
         cs.cl_head = 0u;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Asynchronous drain by warp workers (RunParams::warp_drain = 1).
+//
+// Every warp of a CTA works on its own: it takes up to WQ_BATCH entries (one
+// per lane) from the CTA's shared-memory work queue, relaxes them and pushes
+// the improvements back into the same queue, with no block barrier between
+// batches, so a warp waiting on the L2 round trips of its batch never holds
+// up the others and the next hop of the wavefront starts as soon as its entry
+// is queued. Sources of work, in order: chunks of the CTA's row tasks (rows of
+// more than hub_min_warp selected arcs, worked by all warps of the CTA), the
+// work queue, the CTA's ring range (ring positions its agent took, popped by
+// any warp), and - when all are empty - one poll by the CTA's agent (one warp
+// at a time): chunks of other CTAs' hub rows, a new ring range, and, when the
+// CTA holds no work, the drain's termination.
+//
+// Termination. cs.wq_pending counts the work the CTA holds (queued entries,
+// entries being relaxed, the unrelaxed part of its ring range, open row
+// tasks and chunks being relaxed); the CTA holds one unit of the ring's busy
+// counter exactly while it is non-zero (taken by the warp that raises it from
+// zero, before that warp marks any ring item done; returned by the warp that
+// brings it to zero, after its pushes). Hub records hold their own busy unit
+// until their last chunk is relaxed. The agent of a CTA that holds nothing ends
+// the drain when it reads, in this order, the ring's done count, busy == 0 and
+// the tail equal to that done count: every ring item pushed by then was
+// relaxed, and no CTA held work in between, so no work can appear any more.
+// ---------------------------------------------------------------------------
+constexpr u32 TASK_CHUNK = 128;  // arcs of a row task claimed at a time (4 per lane)
+
+__device__ __forceinline__ unsigned long long vld64_s(const unsigned long long* q) {
+    return *(const volatile unsigned long long*)q;
+}
+__device__ __forceinline__ u32 claim_next(unsigned long long w) { return (u32)(w & 0xFFFFFFull); }
+__device__ __forceinline__ u32 claim_len(unsigned long long w) { return (u32)((w >> 24) & 0xFFFFFFull); }
+__device__ __forceinline__ u32 claim_gen(unsigned long long w) { return (u32)(w >> 48); }
+
+// Returns k units of the CTA's pending work; the warp that brings the count
+// to zero returns the CTA's busy unit (after its pushes are visible). Lane 0.
+__device__ __forceinline__ void pending_done(Coop& cs, u32* aq, u32 k) {
+    if (atomicSub(&cs.wq_pending, k) == k) {
+        __threadfence();
+        atomicSub(aq + AQ_BUSY, 1u);
+    }
+}
+// Adds k units; the warp that raises the count from zero takes a busy unit
+// (visible before anything it marks done). Lane 0.
+__device__ __forceinline__ void pending_take(Coop& cs, u32* aq, u32 k) {
+    if (atomicAdd(&cs.wq_pending, k) == 0u) {
+        atomicAdd(aq + AQ_BUSY, 1u);
+        __threadfence();
+    }
+}
+
+// Prepares the CTA's work queue, ring range and row tasks for a bucket. All threads.
+__device__ __forceinline__ void wq_reset(Coop& cs) {
+    unsigned long long* wq = wq_slots(cs);
+    for (u32 i = threadIdx.x; i < WQ_CAP; i += blockDim.x) wq[i] = RING_FREE;
+    if (threadIdx.x < TASK_CAP) {
+        cs.task[threadIdx.x].claim = 0ull;  // generation 0, nothing to claim
+        cs.task[threadIdx.x].free = 1u;
+    }
+    if (threadIdx.x == 0) {
+        cs.wq_head = cs.wq_tail = cs.wq_pending = 0u;
+        cs.wq_agent = cs.wq_exit = cs.wq_idle = cs.wq_hint = 0u;
+        cs.wq_backoff = 0u;
+        cs.hub_cursor = 0u;
+        cs.task_open = 0u;
+        cs.rr = 0ull;
+    }
+    __syncthreads();
+}
+
+// Reserves up to max_take queued positions [h, h + n). Lane 0.
+__device__ __forceinline__ u32 wq_pop(Coop& cs, u32 max_take, u32& h) {
+    h = vld_s(&cs.wq_head);
+    for (int tries = 0; tries < 64; ++tries) {
+        const int avail = (int)(vld_s(&cs.wq_tail) - h);
+        if (avail <= 0) return 0u;
+        const u32 take = min((u32)avail, max_take);
+        const u32 o = atomicCAS(&cs.wq_head, h, h + take);
+        if (o == h) return take;
+        h = o;
+    }
+    return 0u;
+}
+
+// Pops up to max_take positions [h, h + n) of the CTA's ring range. Lane 0.
+__device__ __forceinline__ u32 rr_pop(Coop& cs, u32 max_take, u32& h) {
+    unsigned long long w = vld64_s(&cs.rr);
+    for (int tries = 0; tries < 64; ++tries) {
+        const u32 lo = (u32)w, hi = (u32)(w >> 32);
+        const int avail = (int)(hi - lo);
+        if (avail <= 0) return 0u;
+        const u32 take = min((u32)avail, max_take);
+        const unsigned long long o = atomicCAS(&cs.rr, w, ((unsigned long long)hi << 32) | (lo + take));
+        if (o == w) {
+            h = lo;
+            return take;
+        }
+        w = o;
+    }
+    return 0u;
+}
+
+// Entry of reserved queue position pos (waits, bounded, for its pusher to
+// write it) and frees the slot.
+__device__ __forceinline__ unsigned long long wq_take(Coop& cs, u32 pos, const RunParams& p) {
+    volatile unsigned long long* slot = wq_slots(cs) + (pos & WQ_MASK);
+    unsigned long long v = *slot;
+    if (v == RING_FREE) {
+        const u64 t0 = global_timer_ns();
+        while ((v = *slot) == RING_FREE) {
+            if (global_timer_ns() - t0 > p.timeout_ns) {
+                flag_timeout(p.ctl, WS_LOCAL_SLOT);
+                return RING_FREE;
+            }
+            __nanosleep(20);
+        }
+    }
+    *slot = RING_FREE;
+    return v;
+}
+
+// Entry of reserved ring position pos (waits, bounded, for its producer) and frees the slot.
+__device__ __forceinline__ unsigned long long ring_take(const RunParams& p, u32 pos) {
+    unsigned long long* slot = p.ring + (pos & p.ring_mask);
+    unsigned long long ent = ld_relaxed64(slot);
+    if (ent == RING_FREE) {
+        const u64 t0 = global_timer_ns();
+        while ((ent = ld_relaxed64(slot)) == RING_FREE) {
+            if (global_timer_ns() - t0 > p.timeout_ns) {
+                flag_timeout(p.ctl, WS_RING_SLOT);
+                return RING_FREE;
+            }
+            __nanosleep(32);
+        }
+    }
+    *slot = RING_FREE;
+    return ent;
+}
+
+// Posts the row [eb, eb + len) of the calling lane's item as a row task of the
+// CTA; false if every task slot is taken. The calling warp holds pending work,
+// so the task's own unit is added without a busy hand-over.
+__device__ __forceinline__ bool task_post(Coop& cs, u32 gi, u32 u, u32 du, u32 ib, u32 inst, u64 ub, u32 eb,
+                                          u32 len) {
+    if (len >= (1u << 24) - TASK_CHUNK) return false;
+    for (u32 i = 0; i < TASK_CAP; ++i) {
+        RowTask& t = cs.task[i];
+        if (vld_s(&t.free) == 0u || atomicCAS(&t.free, 1u, 0u) != 1u) continue;
+        t.gi = gi;
+        t.u = u;
+        t.du = du;
+        t.ib = ib;
+        t.inst = inst;
+        t.ub = ub;
+        t.eb = eb;
+        t.len = len;
+        t.done = 0u;
+        atomicAdd(&cs.wq_pending, 1u);
+        atomicAdd(&cs.task_open, 1u);
+        __threadfence_block();  // fields before the claim word
+        const unsigned long long gen = (unsigned long long)((claim_gen(vld64_s(&t.claim)) + 1u) & 0xFFFFu);
+        atomicExch(&t.claim, (gen << 48) | ((unsigned long long)len << 24));
+        return true;
+    }
+    return false;
+}
+
+// Claims the next chunk [e0, e1) of an open row task; returns its slot or ~0u. Lane 0.
+__device__ __forceinline__ u32 task_claim(Coop& cs, u32& e0, u32& e1) {
+    for (u32 i = 0; i < TASK_CAP; ++i) {
+        RowTask& t = cs.task[i];
+        unsigned long long w = vld64_s(&t.claim);
+        for (int tries = 0; tries < 8; ++tries) {
+            const u32 nx = claim_next(w), len = claim_len(w);
+            if (nx >= len) break;
+            const unsigned long long o = atomicCAS(&t.claim, w, w + TASK_CHUNK);
+            if (o == w) {  // the task cannot complete before this chunk: its fields are stable
+                const u32 eb = vld_s(&t.eb);
+                e0 = eb + nx;
+                e1 = eb + min(len, nx + TASK_CHUNK);
+                return i;
+            }
+            w = o;
+        }
+    }
+    return ~0u;
+}
+
+// Relaxes arcs [e0, e1) of one item with the calling warp, four arcs per lane
+// in flight (so 128 arcs cost one dependent round of state updates).
+template <bool ASTAR, int AM>
+__device__ __forceinline__ void warp_relax_span(const RunParams& p, const Snap& s, u32 u, u32 du, u32 ib, u64 ub,
+                                                u32 inst, u32 e0, u32 e1, Local& L, Coop* cl) {
+    const u32 lane = threadIdx.x & 31u;
+    for (u32 base = e0; base < e1; base += 128u) {
+        u32 hv[4], hw[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const u32 e = base + lane + 32u * (u32)j;
+            uint2 a = make_uint2(0u, PAD_W);
+            if (e < e1) a = __ldg(p.adj + e);
+            hv[j] = a.x;
+            hw[j] = a.y;
+        }
+        relax4<ASTAR, AM>(p, s, u, du, ib, ub, inst, hv, hw, L, cl);
+    }
+}
+
+// A hub chunk is done: the record's busy unit ends with its last chunk
+// (pushes of the chunk are visible first). Lane 0.
+__device__ __forceinline__ void hub_chunk_done(const RunParams& p, u32 k, u32 arcs) {
+    HubRec* r = p.hubs + k;
+    __threadfence();
+    if (atomicAdd(&r->done, arcs) + arcs == __ldcg(&r->ee) - __ldcg(&r->eb)) atomicSub(p.aq + AQ_BUSY, 1u);
+}
+
+// The calling warp works hub record k (just published by one of its lanes, for
+// an item it holds) until no chunk is left; idle CTAs' agents claim chunks too.
+template <bool ASTAR, int AM>
+__device__ __forceinline__ void warp_own_hub(const RunParams& p, const Snap& s, u32 k, u32 u, u32 du, u32 ib, u64 ub,
+                                             u32 inst, Local& L, Coop* cl) {
+    const u32 lane = threadIdx.x & 31u;
+    HubRec* r = p.hubs + k;
+    const u32 eb = __ldcg(&r->eb), len = __ldcg(&r->ee) - eb;
+    for (;;) {
+        u32 off = 0;
+        if (lane == 0) off = atomicAdd(&r->next, p.hub_chunk_warp);
+        off = __shfl_sync(FULL, off, 0);
+        if (off >= len) break;
+        const u32 e1 = min(len, off + p.hub_chunk_warp);
+        warp_relax_span<ASTAR, AM>(p, s, u, du, ib, ub, inst, eb + off, eb + e1, L, cl);
+        __syncwarp();
+        if (lane == 0) hub_chunk_done(p, k, e1 - off);
+    }
+}
+
+enum WarpSrc : u32 { WSRC_NONE = 0, WSRC_LOCAL = 1, WSRC_RANGE = 2, WSRC_HUB = 3, WSRC_TASK = 4, WSRC_EXIT = 5 };
+
+// One poll by the CTA's agent (lane 0 of a warp that found no work; at most one
+// warp of the CTA polls at a time). Returns WSRC_HUB with arcs [e0, e1) of hub
+// record h claimed (counted as pending work), WSRC_RANGE after it installed a
+// new ring range (counted as pending and marked done in the ring), WSRC_EXIT
+// when the bucket is drained or the run failed, WSRC_NONE otherwise.
+__device__ u32 drain_agent(const RunParams& p, const Snap& s, Coop& cs, u32& h, u32& e0, u32& e1) {
+    if (atomicCAS(&cs.wq_agent, 0u, 1u) != 0u) return WSRC_NONE;
+    u32* aq = p.aq;
+    u32 res = WSRC_NONE;
+    if (vload(&p.ctl->rd.status) != DS_OK) res = WSRC_EXIT;
+    if (res == WSRC_NONE && p.hubs) {
+        // chunks of published hub rows (records not yet ready are passed: their publisher works them)
+        const u32 cnt = min(ld_relaxed(aq + AQ_HUBS), p.hub_cap);
+        u32 k = cs.hub_cursor;
+        for (; k < cnt; ++k) {
+            HubRec* r = p.hubs + k;
+            if (ld_acquire(&r->ready) != s.near_epoch) continue;
+            const u32 eb = __ldcg(&r->eb), ee = __ldcg(&r->ee);
+            if (__ldcg(&r->next) >= ee - eb) continue;  // no chunk left
+            const u32 off = atomicAdd(&r->next, p.hub_chunk_warp);
+            if (off < ee - eb) {
+                h = k;
+                e0 = eb + off;
+                e1 = min(ee, e0 + p.hub_chunk_warp);
+                res = WSRC_HUB;
+                break;
+            }
+        }
+        cs.hub_cursor = k;
+        if (res == WSRC_HUB) pending_take(cs, aq, 1u);
+    }
+    if (res == WSRC_NONE && (int)((u32)(vld64_s(&cs.rr) >> 32) - (u32)vld64_s(&cs.rr)) <= 0) {
+        // a new ring range for the CTA's warps: a fair share of the ring, 32 .. blockDim.x items
+        const u32 t = ld_acquire(aq + AQ_TAIL);
+        const u32 hh = ld_relaxed(aq + AQ_HEAD);
+        const int avail = (int)(t - hh);
+        if (avail > 0) {
+            u32 want = ((u32)avail + gridDim.x - 1u) / gridDim.x;
+            want = min(max(want, 32u), blockDim.x);
+            want = min(want, (u32)avail);
+            if (atomicCAS(aq + AQ_HEAD, hh, hh + want) == hh) {
+                pending_take(cs, aq, want);  // busy unit before the items count as done
+                atomicAdd(aq + AQ_DONE, want);
+                atomicExch(&cs.rr, ((unsigned long long)(hh + want) << 32) | hh);
+                res = WSRC_RANGE;
+            }
+        }
+    }
+    if (res == WSRC_RANGE || res == WSRC_HUB) {
+        if (cs.wq_idle) {
+            atomicSub(aq + AQ_IDLE, 1u);
+            cs.wq_idle = 0u;
+        }
+        cs.wq_backoff = 0u;
+    } else if (res == WSRC_NONE) {
+        if (vld_s(&cs.wq_pending) == 0u) {
+            if (!cs.wq_idle) {
+                atomicAdd(aq + AQ_IDLE, 1u);
+                cs.wq_idle = 1u;
+            }
+            // done, then busy, then tail (see above)
+            const u32 d = ld_acquire(aq + AQ_DONE);
+            const u32 b = ld_acquire(aq + AQ_BUSY);
+            const u32 t = ld_acquire(aq + AQ_TAIL);
+            if (b == 0u && d == t) res = WSRC_EXIT;
+        }
+        if (res == WSRC_NONE) {
+            cs.wq_hint = ld_relaxed(aq + AQ_IDLE);
+            const u32 beat = ld_relaxed(aq + AQ_BEAT);
+            if (beat != cs.wq_beat_seen) {  // another CTA made progress: this CTA's waits are not a hang
+                cs.wq_beat_seen = beat;
+                atomicAdd(&cs.wq_beats, 1u);
+            }
+            cs.wq_backoff = min(max(2u * cs.wq_backoff, 32u), 512u);
+        }
+    }
+    if (res == WSRC_EXIT) {
+        cs.wq_exit = 1u;
+        if (cs.wq_idle) {
+            atomicSub(aq + AQ_IDLE, 1u);
+            cs.wq_idle = 0u;
+        }
+    }
+    __threadfence_block();
+    atomicExch(&cs.wq_agent, 0u);
+    return res;
+}
+
+template <bool ASTAR, int AM, int MAP>
+__device__ __forceinline__ void warp_drain(const RunParams& p, const Snap& s, Local& L, Coop& cs, bool busy_held) {
+    const u32 lane = threadIdx.x & 31u;
+    u32* aq = p.aq;
+    Ctl* c = p.ctl;
+    __syncthreads();  // the bucket's scan (if any) has queued its entries
+    if (threadIdx.x == 0) {
+        cs.wq_beats = 0u;
+        cs.wq_beat_seen = 0u;
+        // the busy unit the transition gave this CTA for its scan stays only while the CTA holds work
+        if (busy_held && vld_s(&cs.wq_pending) == 0u) {
+            __threadfence();  // (ring pushes of the scan first)
+            atomicSub(aq + AQ_BUSY, 1u);
+        }
+    }
+    L.spilled = 0u;
+    __syncthreads();
+    // entries per batch: one per lane for 4-slot rows (a batch is one round of
+    // state updates); half a warp otherwise (rows average several arcs each)
+    const u32 B = p.row_stride == ROW_ALIGN ? WQ_BATCH : WQ_BATCH / 2u;
+    bool waiting = false;  // lane 0: the warp is in a wait that started at t0 with progress count `seen`
+    u32 seen = 0u, polls = 0u;
+    u64 t0 = 0ull;
+    for (;;) {
+        u32 src = WSRC_NONE, n = 0, h = 0, e0 = 0, e1 = 0, hint = ~0u;
+        if (lane == 0) {
+            if (vld_s(&cs.wq_exit)) {
+                src = WSRC_EXIT;
+            } else if (vld_s(&cs.task_open) && (h = task_claim(cs, e0, e1)) != ~0u) {
+                src = WSRC_TASK;
+                atomicAdd(&cs.wq_pending, 1u);  // (the open task holds a unit: never from zero)
+            } else if ((n = wq_pop(cs, B, h)) != 0u) {
+                src = WSRC_LOCAL;
+            } else if ((n = rr_pop(cs, B, h)) != 0u) {
+                src = WSRC_RANGE;
+            } else {
+                src = drain_agent(p, s, cs, h, e0, e1);
+                if (src == WSRC_RANGE) {
+                    n = rr_pop(cs, B, h);
+                    if (n == 0u) src = WSRC_NONE;
+                }
+            }
+            if (src == WSRC_NONE) {
+                const u32 b = vld_s(&cs.wq_beats);
+                const u64 now = global_timer_ns();
+                if (!waiting || b != seen) {
+                    waiting = true;
+                    seen = b;
+                    t0 = now;
+                } else if (now - t0 > p.timeout_ns) {
+                    flag_timeout(c, WS_DRAIN_IDLE);
+                    cs.wq_exit = 1u;
+                    src = WSRC_EXIT;
+                }
+                if (src == WSRC_NONE) __nanosleep(max(vld_s(&cs.wq_backoff), 32u));
+            } else if (src != WSRC_EXIT) {
+                waiting = false;
+                if ((++polls & 15u) == 0u) hint = ld_relaxed(aq + AQ_IDLE);  // refresh the spill hint now and then
+            }
+        }
+        src = __shfl_sync(FULL, src, 0);
+        if (src == WSRC_EXIT) break;
+        if (src == WSRC_NONE) continue;
+        n = __shfl_sync(FULL, n, 0);
+        h = __shfl_sync(FULL, h, 0);
+        if (src == WSRC_HUB || src == WSRC_TASK) {
+            e0 = __shfl_sync(FULL, e0, 0);
+            e1 = __shfl_sync(FULL, e1, 0);
+            u32 u, du, ib, inst;
+            u64 ub = ~0ull;
+            if (src == WSRC_TASK) {
+                const RowTask& t = cs.task[h];
+                u = t.u;
+                du = t.du;
+                ib = t.ib;
+                inst = t.inst;
+                if constexpr (ASTAR) ub = t.ub;
+            } else {  // another CTA's hub row: the record's item from its state word
+                const u32 gi = __ldcg(&p.hubs[h].gi);
+                u32 rb;
+                decode_item(p, gi, inst, ib, rb, u);
+                du = st_dist(ld_state(p.state + gi));
+                if constexpr (ASTAR) ub = astar_bound(p, inst, ib);
+            }
+            warp_relax_span<ASTAR, AM>(p, s, u, du, ib, ub, inst, e0, e1, L, &cs);
+            const bool spilled = __any_sync(FULL, L.spilled != 0u);
+            L.spilled = 0u;
+            if (lane == 0) {
+                if (src == WSRC_HUB) {
+                    hub_chunk_done(p, h, e1 - e0);
+                } else {
+                    RowTask& t = cs.task[h];
+                    if (spilled) __threadfence();
+                    if (atomicAdd(&t.done, e1 - e0) + (e1 - e0) == t.len) {  // the row is complete
+                        atomicSub(&cs.task_open, 1u);
+                        __threadfence_block();
+                        atomicExch(&t.free, 1u);
+                        pending_done(cs, aq, 1u);  // the task's unit
+                    }
+                }
+                pending_done(cs, aq, 1u);  // the chunk's unit
+                if ((atomicAdd(&cs.wq_beats, 1u) & 7u) == 0u) atomicAdd(aq + AQ_BEAT, 1u);
+            }
+            continue;
+        }
+        // a batch of entries, one per lane
+        unsigned long long ent = RING_FREE;
+        if (lane < n) ent = src == WSRC_LOCAL ? wq_take(cs, h + lane, p) : ring_take(p, h + lane);
+        u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, inst = 0, rec = ~0u;
+        u64 ub = ~0ull;
+        bool act = false;
+        if (ent != RING_FREE) {
+            const u32 gi = (u32)ent;
+            act = take_item<ASTAR>(p, s, gi, K_LIGHT, L, u, ib, du, ub, inst, eb, ee, false, 0u, 0u,
+                                   (u32)(ent >> 32));
+            if (MAP == 2 && act && ee - eb > p.hub_min_warp) {
+                // long rows: hub records beyond the CTA tier (other CTAs help), row tasks
+                // of this CTA below it; the warp relaxes the row itself only when both are full
+                if (p.hubs && ee - eb > p.hub_min) rec = hub_publish_at(p, s, gi, eb, ee);
+                if (rec != ~0u || task_post(cs, gi, u, du, ib, inst, ub, eb, ee - eb)) act = false;
+            }
+        }
+        if constexpr (MAP == 2) {
+            if (p.row_stride == ROW_ALIGN)
+                relax_quad<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, &cs);
+            else
+                relax_items_warp<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, &cs);
+            // hub rows this warp published: it works them itself (other CTAs' agents help)
+            unsigned pubs = __ballot_sync(FULL, rec != ~0u);
+            while (pubs) {
+                const int l = __ffs(pubs) - 1;
+                pubs &= pubs - 1u;
+                u64 wub = ~0ull;
+                if constexpr (ASTAR) wub = __shfl_sync(FULL, ub, l);
+                warp_own_hub<ASTAR, AM>(p, s, __shfl_sync(FULL, rec, l), __shfl_sync(FULL, u, l),
+                                        __shfl_sync(FULL, du, l), __shfl_sync(FULL, ib, l), wub,
+                                        __shfl_sync(FULL, inst, l), L, &cs);
+            }
+        } else {  // thread / warp per item: warp-local, no block barrier
+            relax_items<ASTAR, AM, MAP>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, &cs, K_LIGHT);
+        }
+        const bool spilled = __any_sync(FULL, L.spilled != 0u);
+        L.spilled = 0u;
+        if (lane == 0) {
+            if (spilled) __threadfence();  // ring pushes are visible before the pending work returns
+            pending_done(cs, aq, n);
+            if ((atomicAdd(&cs.wq_beats, 1u) & 7u) == 0u) atomicAdd(aq + AQ_BEAT, 1u);
+            if (hint != ~0u) cs.wq_hint = hint;
+        }
+    }
+    __syncthreads();  // every warp has left
 }
 
 // ---------------------------------------------------------------------------
@@ -1429,7 +2109,9 @@ __device__ __forceinline__ void grid_barrier(const RunParams& p, Snap& s, Local&
 // ---------------------------------------------------------------------------
 // The persistent kernel.
 // ---------------------------------------------------------------------------
-template <bool ASTAR, int AM, int MAP>
+// WD: asynchronous buckets drained by warp workers (hybrid mapping only; its
+// own instantiation, so the block-synchronous drain's code stays as it is).
+template <bool ASTAR, int AM, int MAP, bool WD = false>
 __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p) {
     __shared__ Snap s;
     // the cooperative-mapping arrays and the claimed list live in dynamic shared
@@ -1485,6 +2167,7 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
         } else if (ph == PH_COMPACT) {
             round_compact(p, s, cs);
         } else if (ph == PH_ASYNC) {
+            if constexpr (WD) wq_reset(cs);
             if (s.in_count) {
                 // bucket start: this CTA's slice of the far pile (in-window items
                 // are relaxed at once, the rest stay far) or of the seeds
@@ -1494,7 +2177,10 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
                     round_items<ASTAR, AM, MAP>(p, s, p.farq[s.far_in], s.in_count, K_SCAN, L, cs);
             }
             // (the transition gave every CTA a busy unit when there is a slice to scan)
-            async_drain<ASTAR, AM, MAP>(p, s, L, cs, s.in_count != 0u);
+            if constexpr (WD)
+                warp_drain<ASTAR, AM, MAP>(p, s, L, cs, s.in_count != 0u);
+            else
+                async_drain<ASTAR, AM, MAP>(p, s, L, cs, s.in_count != 0u);
         }
         grid_barrier(p, s, L, red, sc, s_flag, s_feat, act0, act1);
     }
@@ -1541,23 +2227,35 @@ static KernelFn pick_am_map(int am, int map) {
     }
 }
 
-static const void* kernel_for(bool astar, int am, int map) {
+template <bool A>
+static KernelFn pick_warp_drain(int am) {
+    switch (am) {
+        case 0: return k_persistent<A, 0, 2, true>;
+        case 1: return k_persistent<A, 1, 2, true>;
+        default: return k_persistent<A, 2, 2, true>;
+    }
+}
+
+// wd: the warp-drain instantiation (hybrid mapping only).
+static const void* kernel_for(bool astar, int am, int map, bool wd = false) {
     if (am < 0 || am > 2) am = 0;
     if (map < 0 || map > 2) map = 2;
+    if (wd && map == 2) return astar ? (const void*)pick_warp_drain<true>(am) : (const void*)pick_warp_drain<false>(am);
     return astar ? (const void*)pick_am_map<true>(am, map) : (const void*)pick_am_map<false>(am, map);
 }
 
 // Dynamic shared memory of the persistent kernel (one Coop per CTA); the
 // opt-in above 48 KB is set once per instantiation and device (not a stream
 // operation, so launches inside a stream capture need nothing more).
-static cudaError_t allow_coop_smem(bool astar, int am, int map) {
-    static std::atomic<unsigned> done[64];  // bit (astar, am, map) per device
+static cudaError_t allow_coop_smem(bool astar, int am, int map, bool wd) {
+    static std::atomic<unsigned> done[64];  // bit (wd, astar, am, map) per device
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    const unsigned bit = 1u << ((astar ? 9 : 0) + 3 * am + map);
+    const bool w = wd && map == 2;
+    const unsigned bit = 1u << ((w ? 18 : 0) + (astar ? 9 : 0) + 3 * am + map);
     if (dev < 64 && (done[dev].load() & bit)) return cudaSuccess;
-    e = cudaFuncSetAttribute(kernel_for(astar, am, map), cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(kernel_for(astar, am, map, w), cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)coop_bytes(MAX_BS));
     if (e == cudaSuccess && dev < 64) done[dev].fetch_or(bit);
     return e;
@@ -1572,8 +2270,11 @@ cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, i
     cfg.blockDim = dim3(block);
     if (am < 0 || am > 2) am = 0;
     if (map < 0 || map > 2) map = 2;
-    const void* k = kernel_for(astar, am, map);
-    const cudaError_t ea = allow_coop_smem(astar, am, map);
+    // the warp drain exists for the hybrid mapping only, and its pushes need its kernel
+    if (p.warp_drain && map != 2) return cudaErrorInvalidValue;
+    const bool wd = p.warp_drain != 0u;
+    const void* k = kernel_for(astar, am, map, wd);
+    const cudaError_t ea = allow_coop_smem(astar, am, map, wd);
     if (ea != cudaSuccess) return ea;
     cfg.dynamicSmemBytes = coop_bytes((u32)block);
     cfg.stream = st;
@@ -1586,12 +2287,12 @@ cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, i
     return cudaLaunchKernelExC(&cfg, k, args);
 }
 
-int persistent_blocks_per_sm(bool astar, int am, int map, int block) {
+int persistent_blocks_per_sm(bool astar, int am, int map, int block, bool wd) {
     int nb = 0;
     if (am < 0 || am > 2) am = 0;
     if (map < 0 || map > 2) map = 2;
-    const void* k = kernel_for(astar, am, map);
-    if (allow_coop_smem(astar, am, map) != cudaSuccess ||
+    const void* k = kernel_for(astar, am, map, wd);
+    if (allow_coop_smem(astar, am, map, wd) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block, coop_bytes((u32)block)) != cudaSuccess) {
         cudaGetLastError();
         return 0;

@@ -410,6 +410,22 @@ u32 eager_rounds_for(const pfg_options& o) {
 
 u64 device_timeout_ns() { return (u64)std::max(1, env_int("PFG_TIMEOUT_MS", 2000)) * 1000000ull; }
 
+void configure_drain(RunParams& p, HubRec* hubs, u32 hub_cap, u32 max_deg, u32* aq, int mapping, int block) {
+    p.warp_drain = (p.ring && mapping == PFG_MAP_HYBRID && env_int("PFG_DRAIN", 0) != 0) ? 1u : 0u;
+    // Rows of more than 256 selected arcs are worked by every warp of the CTA
+    // (row tasks); rows beyond the CTA tier (hub_min) also by other CTAs, which
+    // claim 256 arcs of them at a time.
+    p.hub_min_warp = (u32)std::max(32, env_int("PFG_HUB_WARP", 256));
+    p.hub_chunk_warp = 256u;
+    if (p.ring && p.warp_drain && hubs && mapping == PFG_MAP_HYBRID && max_deg > 8u * (u32)block && !p.hubs) {
+        p.hubs = hubs;
+        p.hub_cap = hub_cap;
+        p.hub_min = 8u * (u32)block;
+        p.hub_chunk = 4u * (u32)block;
+        p.aq = aq;
+    }
+}
+
 bool async_buckets_for(const pfg_options& o, int mode) {
     // Delta-stepping only: Frontier relaxation drained as one unbounded
     // asynchronous bucket relaxes 4-6x the arcs of its eager rounds on road grids
@@ -544,6 +560,7 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
         p.hub_chunk = 4u * (u32)block;
         p.aq = s->d_aq;
     }
+    configure_drain(p, s->d_hubs, s->hub_cap, s->max_deg, s->d_aq, map, block);
     const int bps = blocks_per_sm_for(o, astar != 0, map);
     if (bps <= 0) return fail(PFG_ERR_CUDA, "occupancy query failed for block size %d", block);
     const int grid = s->sm_count * bps;
