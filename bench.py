@@ -436,13 +436,22 @@ def extras(g):
     sweep = {}
     Ks = (16, 32, 64, 128, 256)
     srcs_all = pf.uniform_vertices(g.n, max(Ks), SEED)
+    from dataclasses import replace
+    from pathfinding_gpu_b200 import Schedule
     with pf.GpuSolver(g, max(Ks)) as s:
         for K in Ks:
-            o = HEADLINE_OPTIONS()
-            ms = _median_ms(lambda: s.run_state(srcs_all[:K], o, copy=False)[1], 3)
+            # the drain kind and launch shape the autotuner chooses between, timed per batch size
+            cands = {}
+            for sched in (Schedule.Auto, Schedule.Warp):
+                for bsz, bps in ((256, 4), (1024, 1)):
+                    o = replace(HEADLINE_OPTIONS(), schedule=sched, blockSize=bsz, blocksPerSM=bps)
+                    cands[f"{sched.name}/{bsz}x{bps}"] = round(
+                        _median_ms(lambda: s.run_state(srcs_all[:K], o, copy=False)[1], 3), 3)
+            best = min(cands, key=cands.get)
+            ms = cands[best]
             b_alg = K * (16.0 * g.m + 20.0 * g.n)  # grid: every arc and vertex reachable
-            sweep[str(K)] = {"ms": round(ms, 3), "gteps": round(K * g.m / ms / 1e6, 3),
-                             "roofline_frac": round(b_alg / (ms * 1e-3) / 1e9 / peak, 4)}
+            sweep[str(K)] = {"ms": ms, "best": best, "gteps": round(K * g.m / ms / 1e6, 3),
+                             "roofline_frac": round(b_alg / (ms * 1e-3) / 1e9 / peak, 4), "candidates_ms": cands}
     out["grid1000_batch_sweep"] = sweep
     # --- R-MAT scale 20: batched multi-source throughput, learned policy vs fixed automatic Delta ---
     from pathfinding_gpu_b200 import policy as P

@@ -66,9 +66,14 @@ enum pfg_policy_kind { PFG_POLICY_FIXED = 0, PFG_POLICY_LEARNED = 1 };
  * ASYNC:  one drain per bucket: CTAs relax the vertices they claim from their
  *         own shared-memory list and share work through a ring queue, with a
  *         grid barrier only between buckets.
- * AUTO:   ASYNC for Delta-stepping, ROUNDS for Naive and Frontier (serving
- *         steps always run rounds: a step is bounded by a number of rounds). */
-enum pfg_schedule { PFG_SCHEDULE_AUTO = 0, PFG_SCHEDULE_ROUNDS = 1, PFG_SCHEDULE_ASYNC = 2 };
+ * WARP:   ASYNC with the drain worked by warp workers: every warp takes
+ *         entries from its CTA's shared-memory work queue on its own, with no
+ *         block barrier between batches (Hybrid mapping only; other mappings
+ *         run ASYNC). It sustains more throughput on large batches (hundreds of
+ *         instances), ASYNC has the lower latency on small ones.
+ * AUTO:   ASYNC for Delta-stepping, ROUNDS for Naive and Frontier. */
+enum pfg_schedule { PFG_SCHEDULE_AUTO = 0, PFG_SCHEDULE_ROUNDS = 1, PFG_SCHEDULE_ASYNC = 2,
+                    PFG_SCHEDULE_WARP = 3 };
 
 /* Mirrors GpuOptions (reference: include/gpu_sssp.h:42-52) plus `policy`. */
 typedef struct pfg_options {
@@ -85,8 +90,8 @@ typedef struct pfg_options {
                             grid round; -1 = engine default, 0 = off (extension) */
     int32_t blocks_per_sm; /* CTAs of the persistent kernel per SM; 0 = engine
                               default (1024 resident threads per SM) (extension) */
-    int32_t schedule;    /* enum pfg_schedule, default PFG_SCHEDULE_AUTO; ASYNC
-                            applies to Delta-stepping only (extension)          */
+    int32_t schedule;    /* enum pfg_schedule, default PFG_SCHEDULE_AUTO; ASYNC and
+                            WARP apply to Delta-stepping only (extension)       */
 } pfg_options;
 
 /* Mirrors GpuStats (reference: include/gpu_sssp.h:55-65) plus `rounds`. */

@@ -1,5 +1,5 @@
-"""Autotuner of the launch schedule (CTA size, CTAs per SM, atomic mode, eager
-sub-rounds, Delta multiplier) for a given graph and batch.
+"""Autotuner of the launch schedule (CTA size, CTAs per SM, drain kind, atomic mode,
+eager sub-rounds, Delta multiplier) for a given graph and batch.
 
 Coordinate descent over a small discrete space, timing each candidate with the
 engine's own CUDA-event time (median of `reps` runs); results are cached in a
@@ -19,6 +19,7 @@ from typing import Callable, Dict, Optional, Tuple
 from .solver import AtomicMode, Compaction, GpuAlgo, GpuOptions, Mapping, Policy, Schedule
 
 LAUNCH_SHAPES = [(256, 4), (512, 2), (1024, 1)]       # (threads per CTA, CTAs per SM)
+SCHEDULES = [Schedule.Auto, Schedule.Warp]           # asynchronous drains: CTA passes / warp workers
 ATOMICS = [AtomicMode.MinRBA, AtomicMode.MinNoCheck]
 EAGER = [0, 2, 4, 8]
 DELTA_MULT = [0.25, 0.5, 1.0, 2.0, 4.0, 16.0]
@@ -86,13 +87,18 @@ def tune(time_fn: Callable[[GpuOptions], float], base: GpuOptions, auto_delta: i
     best_t = measure(best)
     knobs = []
     knobs.append([replace(best, blockSize=b, blocksPerSM=s) for b, s in LAUNCH_SHAPES])
+    if base.algo == GpuAlgo.DeltaStep:
+        knobs.append([replace(best, schedule=sc) for sc in SCHEDULES])
     knobs.append([replace(best, atomic=a) for a in ATOMICS])
     knobs.append([replace(best, eager=e) for e in EAGER])
     if base.algo == GpuAlgo.DeltaStep:
         knobs.append([replace(best, delta=max(1, int(round(auto_delta * f)))) for f in DELTA_MULT])
+    names = ["blockSize"] + (["schedule"] if base.algo == GpuAlgo.DeltaStep else []) + ["atomic", "eager"] + \
+        (["delta"] if base.algo == GpuAlgo.DeltaStep else [])
     for i, cands in enumerate(knobs):
         # rebuild the candidates on the current best (earlier knobs may have moved)
-        field = {0: ("blockSize", "blocksPerSM"), 1: ("atomic",), 2: ("eager",), 3: ("delta",)}[i]
+        field = {"blockSize": ("blockSize", "blocksPerSM"), "schedule": ("schedule",), "atomic": ("atomic",),
+                 "eager": ("eager",), "delta": ("delta",)}[names[i]]
         for c in cands:
             trial = replace(best, **{f: getattr(c, f) for f in field})
             if trial == best:

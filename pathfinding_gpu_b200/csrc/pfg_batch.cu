@@ -371,7 +371,7 @@ static pfg_status batch_prepare(pfg_batch* b, const pfg_options* opt_in, RunPara
         p.hub_chunk = 4u * (u32)block;
         p.aq = b->d_aq;
     }
-    configure_drain(p, b->d_hubs, b->hub_cap, b->max_deg, b->d_aq, o.mapping, block);
+    configure_drain(p, o.schedule, b->d_hubs, b->hub_cap, b->max_deg, b->d_aq, o.mapping, block);
     const int bps = blocks_per_sm_for(o, false, o.mapping);
     if (bps <= 0) return set_error(PFG_ERR_CUDA, "occupancy query failed for block size %d", block);
     grid = b->sm_count * bps;

@@ -233,7 +233,7 @@ struct RunParams {
     u32 hub_cap;       // records available
     u32 hub_min;       // items with more selected arcs are published as hubs
     u32 hub_chunk;     // arcs per claimed chunk
-    // Asynchronous drains by warp workers (warp_drain = 1): every warp of a CTA
+    // Asynchronous drains by warp workers (warp_drain = 1, PFG_SCHEDULE_WARP): every warp of a CTA
     // takes entries from the CTA's shared-memory work queue on its own, with no
     // block barrier between batches; rows above hub_min_warp selected arcs are
     // worked in chunks by all warps of the CTA (and rows above hub_min by any

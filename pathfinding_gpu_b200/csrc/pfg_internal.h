@@ -45,11 +45,12 @@ u64 device_timeout_ns();
 // Whether a run drains its buckets asynchronously (ring queue + claimed lists).
 bool async_buckets_for(const pfg_options& o, int mode);
 
-// Asynchronous drains: warp workers when PFG_DRAIN is 1, else block-synchronous
-// passes over the CTA's claimed list. Sets RunParams::warp_drain and the warp
-// tier of long rows, and enables the hub records (hubs, hub_cap) for rows above
-// the warp tier's threshold when the run drains asynchronously with the hybrid mapping.
-void configure_drain(RunParams& p, HubRec* hubs, u32 hub_cap, u32 max_deg, u32* aq, int mapping, int block);
+// Asynchronous drains: warp workers for PFG_SCHEDULE_WARP with the Hybrid
+// mapping, else block-synchronous passes over each CTA's claimed list. Sets
+// RunParams::warp_drain and the warp tier of long rows, and enables the hub
+// records (hubs, hub_cap) for the rows beyond the CTA tier.
+void configure_drain(RunParams& p, int schedule, HubRec* hubs, u32 hub_cap, u32 max_deg, u32* aq, int mapping,
+                     int block);
 
 }  // namespace pfg
 

@@ -302,13 +302,7 @@ __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, 
         return;
     }
     if (cl) {
-        // warp-aggregated: one shared atomic per group of converged lanes
-        const unsigned mask = __activemask();
-        const int lane = threadIdx.x & 31;
-        const int leader = __ffs(mask) - 1;
-        u32 base = 0;
-        if (lane == leader) base = atomicAdd(&cl->cl_n, (u32)__popc(mask));
-        const u32 slot = __shfl_sync(mask, base, leader) + __popc(mask & ((1u << lane) - 1u));
+        const u32 slot = atomicAdd(&cl->cl_n, 1u);
         if (slot - cl->cl_head < CL_CAP) {
             cl->cl[slot & (CL_CAP - 1u)] = gv;
             cl->cl_d[slot & (CL_CAP - 1u)] = nd;
@@ -477,26 +471,6 @@ __device__ __forceinline__ void relax4(const RunParams& p, const Snap& s, u32 u,
             after_improve(p, s, ib + hv[j], key, nd[j], inst, L, cl);
         }
     }
-}
-
-// Fixed 4-slot rows (every row of the graph has at most 4 arcs): the lane that
-// holds an item loads its whole row, one 32-byte sector, with two 128-bit loads
-// and updates all its arcs in one round (relax4). eb is the row start; [eb, ee)
-// the selected arcs (ee <= eb + 4).
-template <bool ASTAR, int AM>
-__device__ __forceinline__ void relax_quad(const RunParams& p, const Snap& s, bool act, u32 u, u32 du, u32 ib,
-                                           u64 ub, u32 inst, u32 eb, u32 ee, Local& L, Coop* cl) {
-    uint4 q0 = make_uint4(0u, PAD_W, 0u, PAD_W), q1 = q0;
-    if (act) {
-        const uint4* a4 = reinterpret_cast<const uint4*>(p.adj + eb);
-        q0 = __ldg(a4);
-        q1 = __ldg(a4 + 1);
-    }
-    const u32 cnt = act ? ee - eb : 0u;
-    const u32 hv[4] = {q0.x, q0.z, q1.x, q1.z};
-    const u32 hw[4] = {cnt > 0u ? q0.y : PAD_W, cnt > 1u ? q0.w : PAD_W, cnt > 2u ? q1.y : PAD_W,
-                       cnt > 3u ? q1.w : PAD_W};
-    relax4<ASTAR, AM>(p, s, u, du, ib, ub, inst, hv, hw, L, cl);
 }
 
 // Instance, state base, row base and local vertex of state index gi.
@@ -753,12 +727,9 @@ __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, b
             }
         }
     } else {
-        // 4-slot rows: each lane updates its item's arcs in one round; short rows
-        // only: each warp balances its own items; else the CTA does (no CTA vote
-        // when no row of the graph has more than 32 arcs)
-        if (p.row_stride == ROW_ALIGN && kind != K_HEAVY)
-            relax_quad<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cl);
-        else if (!p.short_rows && __syncthreads_or(act && ee - eb > WARP_ROW_MAX))
+        // short rows only: each warp balances its own items; else the CTA does
+        // (no CTA vote when no row of the graph has more than 32 arcs)
+        if (!p.short_rows && __syncthreads_or(act && ee - eb > WARP_ROW_MAX))
             relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
         else
             relax_items_warp<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cl);
@@ -1470,9 +1441,9 @@ __device__ __forceinline__ void warp_drain(const RunParams& p, const Snap& s, Lo
     }
     L.spilled = 0u;
     __syncthreads();
-    // entries per batch: one per lane for 4-slot rows (a batch is one round of
-    // state updates); half a warp otherwise (rows average several arcs each)
-    const u32 B = p.row_stride == ROW_ALIGN ? WQ_BATCH : WQ_BATCH / 2u;
+    // entries per batch: about 64 selected arcs (one round of paired state updates
+    // over the warp's lanes), between 4 and WQ_BATCH items
+    const u32 B = (u32)max(4.0, min((double)WQ_BATCH, 64.0 / max(1.0, p.avg_deg)));
     bool waiting = false;  // lane 0: the warp is in a wait that started at t0 with progress count `seen`
     u32 seen = 0u, polls = 0u;
     u64 t0 = 0ull;
@@ -1507,7 +1478,7 @@ __device__ __forceinline__ void warp_drain(const RunParams& p, const Snap& s, Lo
                     cs.wq_exit = 1u;
                     src = WSRC_EXIT;
                 }
-                if (src == WSRC_NONE) __nanosleep(max(vld_s(&cs.wq_backoff), 32u));
+                if (src == WSRC_NONE) __nanosleep(max(vld_s(&cs.wq_backoff), 96u));
             } else if (src != WSRC_EXIT) {
                 waiting = false;
                 if ((++polls & 15u) == 0u) hint = ld_relaxed(aq + AQ_IDLE);  // refresh the spill hint now and then
@@ -1576,10 +1547,9 @@ __device__ __forceinline__ void warp_drain(const RunParams& p, const Snap& s, Lo
             }
         }
         if constexpr (MAP == 2) {
-            if (p.row_stride == ROW_ALIGN)
-                relax_quad<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, &cs);
-            else
-                relax_items_warp<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, &cs);
+            // the arcs of the warp's items dealt over its lanes: the arcs of one item sit
+            // in neighbouring lanes, so their loads and state updates share sectors
+            relax_items_warp<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, &cs);
             // hub rows this warp published: it works them itself (other CTAs' agents help)
             unsigned pubs = __ballot_sync(FULL, rec != ~0u);
             while (pubs) {

@@ -435,7 +435,7 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
         p.ring_mask = s->ring_mask;
         p.aq = s->d_aq;
     }
-    configure_drain(p, nullptr, 0u, s->max_deg, s->d_aq, v->opt.mapping, v->block);
+    configure_drain(p, v->opt.schedule, nullptr, 0u, s->max_deg, s->d_aq, v->opt.mapping, v->block);
     cudaError_t le = launch_persistent(p, true, v->opt.atomic, v->opt.mapping, v->block, v->grid, st);
     if (le != cudaSuccess) {
         cudaGetLastError();

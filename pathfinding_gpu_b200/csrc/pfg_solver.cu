@@ -390,7 +390,7 @@ void sanitize_options(pfg_options& o) {
     if (o.block_size < 32 || o.block_size > 1024 || (o.block_size % 32) != 0) o.block_size = 256;
     if (o.mapping < 0 || o.mapping > 2) o.mapping = PFG_MAP_HYBRID;
     if (o.atomic < 0 || o.atomic > 2) o.atomic = PFG_ATOMIC_MIN_RBA;
-    if (o.schedule < 0 || o.schedule > 2) o.schedule = PFG_SCHEDULE_AUTO;
+    if (o.schedule < 0 || o.schedule > 3) o.schedule = PFG_SCHEDULE_AUTO;
 }
 
 int blocks_per_sm_for(const pfg_options& o, bool astar, int map) {
@@ -410,8 +410,9 @@ u32 eager_rounds_for(const pfg_options& o) {
 
 u64 device_timeout_ns() { return (u64)std::max(1, env_int("PFG_TIMEOUT_MS", 2000)) * 1000000ull; }
 
-void configure_drain(RunParams& p, HubRec* hubs, u32 hub_cap, u32 max_deg, u32* aq, int mapping, int block) {
-    p.warp_drain = (p.ring && mapping == PFG_MAP_HYBRID && env_int("PFG_DRAIN", 0) != 0) ? 1u : 0u;
+void configure_drain(RunParams& p, int schedule, HubRec* hubs, u32 hub_cap, u32 max_deg, u32* aq, int mapping,
+                     int block) {
+    p.warp_drain = (p.ring && mapping == PFG_MAP_HYBRID && schedule == PFG_SCHEDULE_WARP) ? 1u : 0u;
     // Rows of more than 256 selected arcs are worked by every warp of the CTA
     // (row tasks); rows beyond the CTA tier (hub_min) also by other CTAs, which
     // claim 256 arcs of them at a time.
@@ -560,7 +561,7 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
         p.hub_chunk = 4u * (u32)block;
         p.aq = s->d_aq;
     }
-    configure_drain(p, s->d_hubs, s->hub_cap, s->max_deg, s->d_aq, map, block);
+    configure_drain(p, o.schedule, s->d_hubs, s->hub_cap, s->max_deg, s->d_aq, map, block);
     const int bps = blocks_per_sm_for(o, astar != 0, map);
     if (bps <= 0) return fail(PFG_ERR_CUDA, "occupancy query failed for block size %d", block);
     const int grid = s->sm_count * bps;

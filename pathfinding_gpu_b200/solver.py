@@ -56,6 +56,7 @@ class Schedule(IntEnum):
     Auto = 0    # Async for Delta-stepping, Rounds for Naive and Frontier
     Rounds = 1  # relaxation rounds separated by grid barriers (the reference's loop)
     Async = 2   # one drain per bucket through CTA claimed lists and a ring queue
+    Warp = 3    # Async, the drain worked by independent warps (Hybrid mapping)
 
 
 @dataclass

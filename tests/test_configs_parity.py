@@ -86,7 +86,8 @@ def test_rmat20_three_sources_word_for_word(oracle):
     refs = {s: oracle.sssp_canonical(g, s) for s in srcs}
     with pf.GpuSolver(g, 3) as s:
         for src in srcs:
-            for o in (GpuOptions(), GpuOptions(blockSize=1024, atomic=AtomicMode.MinNoCheck)):
+            for o in (GpuOptions(), GpuOptions(blockSize=1024, atomic=AtomicMode.MinNoCheck),
+                      GpuOptions(schedule=Schedule.Warp)):
                 r = s.sssp(src, o)
                 _check(oracle, g, src, r.dist, r.parent, refs[src], ("rmat20", o.blockSize))
         _, _, state = s.run_state(srcs, GpuOptions())

@@ -49,7 +49,8 @@ def test_grid1000_64_sources(oracle):
     srcs = pf.uniform_vertices(g.n, 64, 2026).tolist()
     A = arcs(g)
     with pf.GpuSolver(g, 64) as s:
-        for opt in (GpuOptions(atomic=AtomicMode.MinNoCheck), GpuOptions(schedule=Schedule.Rounds)):
+        for opt in (GpuOptions(atomic=AtomicMode.MinNoCheck), GpuOptions(schedule=Schedule.Rounds),
+                    GpuOptions(atomic=AtomicMode.MinNoCheck, schedule=Schedule.Warp, blockSize=1024)):
             _, _, state = s.run_state(srcs, opt)
             dist, parent = pf.unpack(state)
             for i, src in enumerate(srcs):
@@ -65,7 +66,8 @@ def test_rmat20(oracle):
     A = arcs(g)
     srcs = pf.pick_sources(g, 3, 2026).tolist()
     with pf.GpuSolver(g, 3) as s:
-        for opt in (GpuOptions(blockSize=1024), GpuOptions(), GpuOptions(delta=16, schedule=Schedule.Rounds)):
+        for opt in (GpuOptions(blockSize=1024), GpuOptions(), GpuOptions(delta=16, schedule=Schedule.Rounds),
+                    GpuOptions(schedule=Schedule.Warp), GpuOptions(schedule=Schedule.Warp, delta=16)):
             _, _, state = s.run_state(srcs, opt)
             dist, parent = pf.unpack(state)
             for i, src in enumerate(srcs):
@@ -74,7 +76,7 @@ def test_rmat20(oracle):
         assert np.array_equal(dist[:g.n], d_ref) and np.array_equal(parent[:g.n], p_can)
 
 
-@pytest.mark.parametrize("schedule", [Schedule.Async, Schedule.Rounds])
+@pytest.mark.parametrize("schedule", [Schedule.Async, Schedule.Rounds, Schedule.Warp])
 def test_uneven_batch_full_size(schedule):
     from pathfinding_gpu_b200.batch import GpuBatch
     big = pf.grid(1024, 1024, 2026)

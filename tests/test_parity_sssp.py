@@ -67,7 +67,7 @@ def test_grid100_all_sources(oracle, grid100, grid100_solver, algo):
         check_sssp(oracle, grid100, src, res)
 
 
-SCHEDULES = [Schedule.Rounds, Schedule.Async]
+SCHEDULES = [Schedule.Rounds, Schedule.Async, Schedule.Warp]
 
 
 @pytest.mark.parametrize("mapping,atomic", list(itertools.product(list(Mapping), list(AtomicMode))))
@@ -95,17 +95,18 @@ def test_async_buckets_take_one_barrier_per_bucket(grid100_solver):
 
 @pytest.mark.parametrize("block", [32, 256, 1024])
 def test_grid300_async_batch(oracle, block):
-    # wider wavefronts: claimed lists overflow and spill into the ring
+    # wider wavefronts: claimed lists / work queues overflow and spill into the ring
     g = pf.grid(300, 300, SEED)
     srcs = pf.uniform_vertices(g.n, 8, SEED + 3).tolist()
+    refs = [oracle.sssp_canonical(g, src) for src in srcs]
     with pf.GpuSolver(g, 8) as s:
         for atomic in (AtomicMode.MinRBA, AtomicMode.MinNoCheck):
-            _, _, state = s.run_state(srcs, GpuOptions(blockSize=block, atomic=atomic, schedule=Schedule.Async))
-            dist, parent = pf.unpack(state)
-            for i, src in enumerate(srcs):
-                d_ref, p_can = oracle.sssp_canonical(g, src)
-                assert np.array_equal(dist[i * g.n:(i + 1) * g.n], d_ref), (block, atomic, i)
-                assert np.array_equal(parent[i * g.n:(i + 1) * g.n], p_can), (block, atomic, i)
+            for sched in (Schedule.Async, Schedule.Warp):
+                _, _, state = s.run_state(srcs, GpuOptions(blockSize=block, atomic=atomic, schedule=sched))
+                dist, parent = pf.unpack(state)
+                for i, (d_ref, p_can) in enumerate(refs):
+                    assert np.array_equal(dist[i * g.n:(i + 1) * g.n], d_ref), (block, atomic, sched, i)
+                    assert np.array_equal(parent[i * g.n:(i + 1) * g.n], p_can), (block, atomic, sched, i)
 
 
 @pytest.mark.parametrize("eager", [0, 1, 3, 16, 64])
