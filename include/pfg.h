@@ -308,7 +308,11 @@ PFG_API pfg_solver* pfg_server_solver(pfg_server* v);
 PFG_API pfg_status pfg_set_policy(pfg_solver* s, const float* params, uint64_t count);
 PFG_API uint64_t pfg_policy_param_count(void);
 /* A Delta-stepping run (fixed or learned Delta) that also returns, for every
- * bucket advance, one trace row of 16 floats: the 12 policy features, then
+ * decision point (the first bucket and every bucket advance), one trace row of
+ * 16 floats: the 12 policy features (log2 frontier size, log2 items and log2
+ * arcs of the last bucket, its work ratio, the degree histogram of a frontier
+ * sample in three bins, its light-arc fraction, its distance spread / Delta,
+ * the gap to the next key / avgW, log2 Delta / avgW, log2 buckets so far), then
  * the bucket index, the Delta of the bucket that ended, the items that entered
  * it and the rounds it took. *rows_out = rows written (<= trace_cap). */
 PFG_API pfg_status pfg_run_traced(pfg_solver* s, const uint32_t* h_srcs, uint32_t k,

@@ -242,7 +242,9 @@ struct RunParams {
     u32 warp_drain;
     u32 hub_min_warp;
     u32 hub_chunk_warp;
-    u32 pad_wd;
+    // Block-synchronous drain: claimed-list entries a CTA keeps beyond its pass
+    // before it spills the rest to the ring while no CTA is idle (0: half a block).
+    u32 spill_keep;
 };
 
 // ---------------------------------------------------------------------------

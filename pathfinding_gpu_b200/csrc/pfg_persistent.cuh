@@ -939,7 +939,7 @@ __device__ __forceinline__ void async_drain(const RunParams& p, const Snap& s, L
                 h = cs.cl_head;
                 n = local < BS ? local : BS;
                 const u32 backlog = local - n;
-                const u32 keep = BS / 2u;
+                const u32 keep = p.spill_keep ? p.spill_keep : BS / 2u;
                 if (backlog >= 32u && (s_idle > 0u || backlog > keep))
                     spill = s_idle > 0u ? backlog / 2u : backlog - keep;
                 cs.cl_head = h + n;
@@ -1697,39 +1697,87 @@ static __device__ u32 policy_pick(const PolicyNet* net, const float* feat, float
 // asks for it).
 // ---------------------------------------------------------------------------
 // Features of a decision point (the start of the first bucket, or a bucket
-// advance), computed by thread 0 of the transition CTA:
-//   0 log2(1 + items of the next bucket's input)   6 log2(Delta / avgW)
-//   1 log2(1 + items that entered the last bucket) 7 log2(1 + avgDeg)
-//   2 log2(1 + rounds of the last bucket)          8 log2(maxW / avgW)
-//   3 (next smallest key - window end) / avgW      9 log2(1 + n)
-//   4 log2(1 + arcs scanned in the last bucket)   10 next smallest key / (avgW sqrt(n))
-//   5 log2(1 + buckets so far)                    11 min(1, Delta / maxW)
-// With tracing on, the row is also written to p.trace (decision k -> row k).
-static __device__ void decision_features(const RunParams& p, Ctl& sc, const Rd& r, u32 fn, u64 est, float* f) {
+// advance). Thread 0 of the transition CTA computes the counters, then the whole
+// CTA samples the frontier (frontier_sample):
+//   0 log2(1 + items of the next bucket's input: the frontier)
+//   1 log2(1 + items that entered the last bucket)
+//   2 log2(1 + arcs scanned in the last bucket)
+//   3 work ratio of the last bucket: arcs scanned / (items x average degree)
+//   4 5 6 degree histogram of the sampled frontier: rows of <= 4, 5..32, > 32 slots
+//   7 light fraction of the sampled rows' arcs (w <= Delta of the bucket that ended)
+//   8 spread of the sampled tentative distances, (max - min) / Delta
+//   9 gap between the frontier's smallest key and the window end, / avgW
+//  10 log2(Delta / avgW)
+//  11 log2(1 + buckets so far)
+// s_flag[3..7] hand the sample over: requested, queue kind (0 near queue 0 /
+// 1 far pile), far pile index, item count, Delta. With tracing on, the row is
+// written to p.trace (decision k -> row k) after the sample.
+static __device__ void decision_features(const RunParams& p, Ctl& sc, const Rd& r, u32 fn, u64 est, float* f,
+                                         u32* s_flag, u32 far_pile) {
     const double aw = p.avg_w > 0.0 ? p.avg_w : 1.0;
     const u64 edges_now = sc.bucket_edges_acc;
+    const double arcs = (double)(edges_now - sc.bucket_edges);
     f[0] = log2f(1.f + (float)fn);
     f[1] = log2f(1.f + (float)sc.bucket_near);
-    f[2] = log2f(1.f + (float)sc.bucket_rounds);
-    f[3] = (float)((double)(est > r.hi ? est - r.hi : 0ull) / aw);
-    f[4] = log2f(1.f + (float)(edges_now - sc.bucket_edges));
-    f[5] = log2f(1.f + (float)sc.buckets);
-    f[6] = log2f((float)((double)r.delta / aw));
-    f[7] = log2f(1.f + (float)p.avg_deg);
-    f[8] = log2f((float)((double)p.maxw / aw));
-    f[9] = log2f(1.f + (float)p.n);
-    f[10] = (float)((double)est / (aw * sqrt((double)p.n)));
-    f[11] = fminf(1.f, (float)r.delta / (float)(p.maxw ? p.maxw : 1u));
+    f[2] = log2f(1.f + (float)arcs);
+    f[3] = fminf(64.f, (float)(arcs / fmax(1.0, (double)sc.bucket_near * fmax(1.0, p.avg_deg))));
+    f[9] = (float)((double)(est > r.hi ? est - r.hi : 0ull) / aw);
+    f[10] = log2f((float)((double)r.delta / aw));
+    f[11] = log2f(1.f + (float)sc.buckets);
     sc.bucket_edges = edges_now;
-    const u32 row = sc.buckets;
-    if (p.trace && row < p.trace_cap) {
-        float* tr = p.trace + (size_t)row * TRACE_W;
-        for (int i = 0; i < POL_IN; ++i) tr[i] = f[i];
-        tr[POL_IN + 0] = (float)sc.buckets;
-        tr[POL_IN + 1] = (float)r.delta;
-        tr[POL_IN + 2] = (float)sc.bucket_near;
-        tr[POL_IN + 3] = (float)sc.bucket_rounds;
+    s_flag[3] = 1u;
+    s_flag[4] = far_pile == ~0u ? 0u : 1u;
+    s_flag[5] = far_pile == ~0u ? 0u : far_pile;
+    s_flag[6] = fn;
+    s_flag[7] = r.delta;
+}
+
+// The sampled features 4..8 of a decision point: up to 64 items of the frontier
+// (evenly spaced in its queue), their row lengths, light arcs and distances.
+// Called by every thread of the transition CTA.
+static __device__ void frontier_sample(const RunParams& p, const u32* q, u32 cnt, u32 delta, float* f) {
+    __shared__ u32 s_bin[4], s_slots, s_dmin, s_dmax;
+    const u32 t = threadIdx.x;
+    if (t == 0) {
+        s_bin[0] = s_bin[1] = s_bin[2] = s_bin[3] = 0u;
+        s_slots = 0u;
+        s_dmin = INF32;
+        s_dmax = 0u;
     }
+    __syncthreads();
+    const u32 S = min(cnt, min(64u, blockDim.x));
+    if (t < S) {
+        const u32 gi = ld_cg(q + (u32)(((u64)t * cnt) / S));
+        u32 inst, ib, rb, u;
+        decode_item(p, gi, inst, ib, rb, u);
+        u32 r0, r1;
+        if (p.row_stride) {
+            r0 = (rb ? __ldg(p.prow + rb) : 0u) + ROW_ALIGN * u;
+            r1 = r0 + ROW_ALIGN;
+        } else {
+            r0 = __ldg(p.prow + rb + u);
+            r1 = __ldg(p.prow + rb + u + 1);
+        }
+        const u32 slots = r1 - r0;
+        atomicAdd(&s_bin[slots <= 4u ? 0 : (slots <= 32u ? 1 : 2)], 1u);
+        atomicAdd(&s_bin[3], light_end(p.adj, r0, r1, delta) - r0);
+        atomicAdd(&s_slots, slots);
+        const u32 d = st_dist(ld_state(p.state + gi));
+        if (d != INF32) {
+            atomicMin(&s_dmin, d);
+            atomicMax(&s_dmax, d);
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        const float inv = S ? 1.f / (float)S : 0.f;
+        f[4] = (float)s_bin[0] * inv;
+        f[5] = (float)s_bin[1] * inv;
+        f[6] = (float)s_bin[2] * inv;
+        f[7] = s_slots ? (float)s_bin[3] / (float)s_slots : 1.f;
+        f[8] = s_dmin != INF32 ? fminf(64.f, (float)(s_dmax - s_dmin) / (float)(delta ? delta : 1u)) : 0.f;
+    }
+    __syncthreads();
 }
 
 // Turns the bucket that starts now into an asynchronous one: every CTA scans
@@ -1760,6 +1808,7 @@ static __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, floa
     if (t == 0) {
         Rd& r = sc.rd;
         s_flag[0] = 0;
+        s_flag[3] = 0;
         if (p.hubs) p.aq[AQ_HUBS] = 0u;  // hub records live for one round / bucket drain
         const u32 ph = r.phase;
         const u32 rounds = sc.rounds;
@@ -1821,7 +1870,7 @@ static __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, floa
                 if (p.mode == MODE_DELTA && (p.policy || p.trace)) {
                     // The first bucket is a decision point too: features of the
                     // seed window (nothing relaxed yet) and the graph.
-                    decision_features(p, sc, r, p.k, key0, s_feat);
+                    decision_features(p, sc, r, p.k, key0, s_feat, s_flag, ~0u);
                     if (p.policy) {
                         s_flag[0] = 3u;  // choose the first bucket's Delta below
                         s_key0 = key0;
@@ -1913,7 +1962,7 @@ static __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, floa
                 r.phase = PH_DONE;
             } else {
                 s_flag[0] = p.policy ? 1u : 2u;
-                if (p.policy || p.trace) decision_features(p, sc, r, fn, est, s_feat);
+                if (p.policy || p.trace) decision_features(p, sc, r, fn, est, s_feat, s_flag, fin);
             }
             s_flag[2] = p.inst_far_cnt ? 1u : 0u;
         } else {
@@ -1935,6 +1984,19 @@ static __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, floa
             p.inst_far_cnt[i] = 0u;
         }
         __threadfence();
+    }
+    if (s_flag[3]) {
+        // the frontier sample of the decision point, then its trace row
+        frontier_sample(p, s_flag[4] ? p.farq[s_flag[5]] : p.nearq[0], s_flag[6], s_flag[7], s_feat);
+        const u32 row = sc.buckets;
+        if (t == 0 && p.trace && row < p.trace_cap) {
+            float* tr = p.trace + (size_t)row * TRACE_W;
+            for (int i = 0; i < POL_IN; ++i) tr[i] = s_feat[i];
+            tr[POL_IN + 0] = (float)sc.buckets;
+            tr[POL_IN + 1] = (float)sc.rd.delta;
+            tr[POL_IN + 2] = (float)sc.bucket_near;
+            tr[POL_IN + 3] = (float)sc.bucket_rounds;
+        }
     }
     const u32 need = s_flag[0];
     if (need == 1u || need == 3u) {
@@ -2103,7 +2165,7 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
     Coop& cs = *reinterpret_cast<Coop*>(pfg_dyn_smem);
     __shared__ Ctl sc;
     __shared__ u64 red[32];
-    __shared__ u32 s_flag[3];
+    __shared__ u32 s_flag[8];
     __shared__ float s_feat[POL_IN];
     __shared__ float act0[POL_H], act1[POL_H];
     Local L;

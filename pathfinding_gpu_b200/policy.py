@@ -1,8 +1,12 @@
 """Learned Delta policy: trace collection, training and inference (GPU kernels in pfg_policy.cu).
 
 At every decision point of Delta-stepping (the first bucket and every bucket
-advance) the persistent kernel computes 12 features of the frontier and the
-graph (see decision_features in pfg_kernels.cu) and, with the policy loaded,
+advance) the persistent kernel computes 12 features of the frontier: the size of
+the next bucket's input, the last bucket's items, arcs scanned and work ratio, and
+from a sample of up to 64 frontier items their degree histogram (<= 4, 5-32, > 32
+slots), the fraction of light arcs at the current Delta and the spread of their
+tentative distances, plus the gap to the next key, Delta / avgW and the bucket
+count (decision_features / frontier_sample in pfg_persistent.cuh); with the policy loaded it
 evaluates a 12 -> 64 -> 64 -> 64 -> 16 MLP whose argmax c picks how the next
 bucket runs: Delta = MULTIPLIERS[c % 8] x the automatic Delta, drained
 asynchronously (c < 8) or in relaxation rounds (c >= 8). The policy changes the

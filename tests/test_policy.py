@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import pathfinding_gpu_b200 as pf
-from pathfinding_gpu_b200 import GpuOptions, Policy
+from pathfinding_gpu_b200 import Schedule, GpuOptions, Policy
 from pathfinding_gpu_b200 import policy as P
 from oracle import policy_oracle as PO
 
@@ -88,15 +88,39 @@ def _ratios(oracle, g, srcs, block):
     return out
 
 
+def _static_ceiling(g, srcs, block):
+    """Fixed time / time of the best static class (one Delta multiplier and schedule for
+    every bucket), per source: the most any choice of the policy's classes held for a
+    whole run could gain."""
+    out = []
+    with pf.GpuSolver(g, 1) as s:
+        auto = s.autoDelta()
+        for src in srcs:
+            med = lambda o: statistics.median(s.run_state([src], o, copy=False)[1] for _ in range(3))
+            s.run_state([src], GpuOptions(blockSize=block), copy=False)
+            tf = med(GpuOptions(blockSize=block))
+            best = min(med(GpuOptions(blockSize=block, delta=max(1, int(np.float32(auto) * np.float32(mult))),
+                                      schedule=Schedule.Async if c < 8 else Schedule.Rounds))
+                       for c, mult in enumerate(P.MULTIPLIERS * 2))
+            out.append(tf / best)
+    return out
+
+
 @pytest.mark.skipif(not P.WEIGHTS.exists(), reason="trained weights not present")
 def test_trained_policy_gain_on_unseen_graphs(oracle):
     # Graphs never trained on, median over three sources of fixed automatic
-    # Delta time / learned time. The 1000 x 1000 grid gains from the larger
-    # Deltas the network picks; on R-MAT scale 20 the fixed engine is already
-    # within ~1.25x of the best class, so the bar there is "no loss".
+    # Delta time / learned time, results compared word for word. The 1000 x 1000
+    # grid gains from the larger Deltas the network picks. On R-MAT scale 20 the
+    # measured ceiling of the policy's classes - the best static class per source -
+    # is about 1.05x over the fixed automatic Delta (the fixed run covers the graph
+    # in three buckets), far below 1.5x: the bar there is most of that ceiling and
+    # no loss against the fixed form.
     grid = pf.grid(1000, 1000, 2026)
     r_grid = _ratios(oracle, grid, pf.pick_sources(grid, 3, 99).tolist(), 1024)
     assert statistics.median(r_grid) >= 1.08, r_grid
     rmat = pf.rmat(20, 16, seed=2026)
-    r_rmat = _ratios(oracle, rmat, pf.pick_sources(rmat, 3, 2026).tolist(), 1024)
-    assert statistics.median(r_rmat) >= 0.9, r_rmat
+    srcs = pf.pick_sources(rmat, 3, 2026).tolist()
+    r_rmat = _ratios(oracle, rmat, srcs, 1024)
+    ceiling = _static_ceiling(rmat, srcs, 1024)
+    assert statistics.median(r_rmat) >= 0.9, (r_rmat, ceiling)
+    assert statistics.median(r_rmat) >= 0.85 * statistics.median(ceiling), (r_rmat, ceiling)
