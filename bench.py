@@ -465,8 +465,14 @@ def extras(g):
         reach = dist != 0xFFFFFFFF
         m_r = int((deg[None, :] * reach).sum())
         n_r = int(reach.sum())
-        ms = _median_ms(lambda: s.run_state(rsrcs, o, copy=False)[1], 3)
-        out["rmat20_batch16"] = {"ms": round(ms, 3), "gteps": round(m_r / ms / 1e6, 3),
+        shapes = {}
+        for sched in (Schedule.Auto, Schedule.Warp):
+            for bsz, bps in ((256, 4), (1024, 1)):
+                oo = replace(o, schedule=sched, blockSize=bsz, blocksPerSM=bps)
+                shapes[f"{sched.name}/{bsz}x{bps}"] = round(_median_ms(lambda: s.run_state(rsrcs, oo, copy=False)[1], 3), 3)
+        best = min(shapes, key=shapes.get)
+        ms = shapes[best]
+        out["rmat20_batch16"] = {"ms": ms, "best": best, "candidates_ms": shapes, "gteps": round(m_r / ms / 1e6, 3),
                                  "roofline_frac": round((16.0 * m_r + 20.0 * n_r) / (ms * 1e-3) / 1e9 / peak, 4),
                                  "reachable_arcs": m_r}
     if P.WEIGHTS.exists():
@@ -517,18 +523,29 @@ def extras(g):
                                "run_ms": round(run_ms, 3), "replay_ms": round(rep_ms, 3),
                                "gteps_replay": round(arcs / rep_ms / 1e6, 3)}
     # --- A* serving with continuous batching on the 2048x2048 road-like graph ---
+    # Poisson arrivals swept over 1k..100k queries/s, slots sized by device memory, the
+    # learned policy on (and the fixed automatic Delta as the fallback it replaces).
     from pathfinding_gpu_b200.serving import GpuServer, run_poisson
+    from pathfinding_gpu_b200 import policy as P
     road = pf.road(2048, seed=SEED)
-    v = pf.uniform_vertices(road.n, 2 * 2000, SEED)
-    qs = [(int(v[2 * i]), int(v[2 * i + 1])) for i in range(2000)]
-    out["serving_road2048"] = {"slots": 128, "bucket_drains_per_step": 8}
-    with GpuServer(road, slots=128) as srv:
-        run_poisson(srv, qs[:50], 1000.0, max_rounds=8, seed=2)  # warm
-        for rate in (1000, 2000):
-            rep = run_poisson(srv, qs[:rate], float(rate), max_rounds=8, seed=3, time_limit_s=30)
-            rep.pop("results")
-            out["serving_road2048"][f"{rate}_qps"] = {k: (round(x, 3) if isinstance(x, float) else x)
-                                                     for k, x in rep.items()}
+    v = pf.uniform_vertices(road.n, 2 * 4000, SEED)
+    qs = [(int(v[2 * i]), int(v[2 * i + 1])) for i in range(4000)]
+    serving = {"graph": f"road 2048x2048, n={road.n}, m={road.m}", "bucket_drains_per_step": 8}
+    for mode in ("learned", "fixed"):
+        opt = GpuOptions(policy=Policy.Learned) if mode == "learned" else GpuOptions()
+        with GpuServer(road, slots=0, opt=opt) as srv:
+            if mode == "learned" and P.WEIGHTS.exists():
+                srv.set_policy(P.load())
+            serving["slots"] = srv.slots
+            run_poisson(srv, qs[:64], 1000.0, max_rounds=8, seed=2)  # warm
+            rates = {}
+            for rate in (1000, 2000, 5000, 10000, 20000, 50000, 100000):
+                k = min(len(qs), max(1000, rate // 2))
+                rep = run_poisson(srv, qs[:k], float(rate), max_rounds=8, seed=3, time_limit_s=20)
+                rep.pop("results")
+                rates[f"{rate}_qps"] = {kk: (round(x, 3) if isinstance(x, float) else x) for kk, x in rep.items()}
+            serving[mode] = rates
+    out["serving_road2048"] = serving
     out["extras_wall_s"] = round(time.perf_counter() - t0, 1)
     return out
 

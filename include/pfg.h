@@ -271,7 +271,15 @@ PFG_API uint64_t pfg_batch_device_bytes(const pfg_batch* b);
  * shared bucket sequence at its next bucket), and retires the slots whose
  * search is complete. Finished queries are drained with pfg_server_results;
  * times are microseconds since the server was created. dist is the exact
- * shortest distance (PFG_INF if unreachable). */
+ * shortest distance (PFG_INF if unreachable). slots = 0 at creation admits by
+ * device memory: the server takes as many slots as fit in 60 % of the device's
+ * free memory after the graph (at most 2048, and slots * n < 2^32); each slot
+ * holds a packed state word, five queue words, three stamp words and two ring
+ * entries per vertex. max_rounds counts bucket drains when the buckets run
+ * asynchronously (the default schedule), relaxation rounds otherwise. With
+ * opt->policy = PFG_POLICY_LEARNED and a network loaded on the server's solver
+ * (pfg_set_policy on pfg_server_solver), the policy picks the shared bucket
+ * sequence's Delta; without a network the fixed automatic Delta is used. */
 typedef struct pfg_server pfg_server;
 typedef struct pfg_query_result {
     uint64_t id;
@@ -291,6 +299,8 @@ PFG_API pfg_status pfg_server_results(pfg_server* v, pfg_query_result* out, uint
                                       uint32_t* n_out);
 PFG_API uint32_t pfg_server_pending(const pfg_server* v);
 PFG_API uint32_t pfg_server_in_flight(const pfg_server* v);
+/* Query slots of the server (the number chosen when it was created with slots = 0). */
+PFG_API uint32_t pfg_server_slots(const pfg_server* v);
 PFG_API double pfg_server_now_us(const pfg_server* v);
 /* The server's solver (graph + slots), e.g. to load a policy network. */
 PFG_API pfg_solver* pfg_server_solver(pfg_server* v);

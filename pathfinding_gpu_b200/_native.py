@@ -67,6 +67,7 @@ SIGNATURES = {
     "pfg_server_results": (i32, [C.c_void_p, P(PfgQueryResult), u32, P(u32)]),
     "pfg_server_pending": (u32, [C.c_void_p]),
     "pfg_server_in_flight": (u32, [C.c_void_p]),
+    "pfg_server_slots": (u32, [C.c_void_p]),
     "pfg_server_now_us": (f64, [C.c_void_p]),
     "pfg_server_solver": (C.c_void_p, [C.c_void_p]),
     # include/pfg.h

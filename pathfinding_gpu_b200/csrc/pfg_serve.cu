@@ -28,6 +28,9 @@ using namespace pfg;
 
 namespace {
 
+// Most slots an automatically sized server takes (slots = 0 at creation).
+constexpr u64 kMaxAutoSlots = 2048;
+
 struct Request {
     uint64_t id;
     uint32_t src, dst;
@@ -41,13 +44,20 @@ struct SlotInfo {
     uint32_t admit_round = 0;
 };
 
-// State words of the admitted slots back to (INF, NO_PARENT).
-__global__ void k_serve_clear(u64* state, const u32* slots, u32 m, u32 n) {
-    const u64 total = (u64)m * n;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (u64)gridDim.x * blockDim.x) {
-        const u32 j = (u32)(i / n);
-        state[(u64)slots[j] * n + (i - (u64)j * n)] = STATE_INIT;
-    }
+// State words of the admitted slots back to (INF, NO_PARENT): blockIdx.y is the
+// admitted slot, the x blocks stream its n words with 16-byte stores (a slot's
+// range starts at a multiple of n words, so its first word may sit mid-pair).
+__global__ void k_serve_clear(u64* state, const u32* slots, u32 n) {
+    u64* base = state + (u64)slots[blockIdx.y] * n;
+    const u32 head = (u32)(((uintptr_t)base >> 3) & 1u);  // one word up to a 16-byte boundary
+    const u32 stride = gridDim.x * blockDim.x;
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (head && t == 0 && n > 0) base[0] = STATE_INIT;
+    const u32 body = n > head ? (n - head) / 2u : 0u;
+    ulonglong2* v = reinterpret_cast<ulonglong2*>(base + head);
+    for (u32 i = t; i < body; i += stride) v[i] = make_ulonglong2(STATE_INIT, STATE_INIT);
+    const u32 tail = head + 2u * body;
+    if (t == 0 && tail < n) base[tail] = STATE_INIT;
 }
 
 struct AdmitParams {
@@ -277,8 +287,34 @@ extern "C" pfg_status pfg_server_create(const uint32_t* row, const uint32_t* col
                                         const double* x, const double* y, uint32_t n, uint32_t m,
                                         double h_scale, double avg_w, double avg_deg, uint32_t slots,
                                         const pfg_options* opt, int32_t device, pfg_server** out) {
-    if (!out || slots == 0) return set_error(PFG_ERR_INVALID_ARGUMENT, "pfg_server_create: bad argument");
+    if (!out || n == 0) return set_error(PFG_ERR_INVALID_ARGUMENT, "pfg_server_create: bad argument");
     *out = nullptr;
+    if (slots == 0) {
+        // Admission by device memory: as many slots as fit in 60 % of the free
+        // memory after the graph (per slot: the packed state, five queues, three
+        // stamp words and its share of the power-of-two ring, of 2 entries per state).
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count || cudaSetDevice(device) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(PFG_ERR_NO_DEVICE, "CUDA device %d not available", device);
+        }
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(PFG_ERR_CUDA, "cudaMemGetInfo failed");
+        }
+        const u64 graph_b = 8ull * ((u64)m + 3ull * n) + 32ull * n;
+        const double budget = 0.6 * (double)(free_b > graph_b ? free_b - graph_b : 0);
+        auto bytes_for = [&](u64 S) {
+            u64 ring = 1024;
+            while (ring < 2 * S * n && ring < (1ull << 32)) ring <<= 1;
+            return (double)S * n * 40.0 + (double)ring * 8.0;
+        };
+        const u64 cap = std::min<u64>(kMaxAutoSlots, (0xFFFFFFFEull / n));
+        u64 S = 1;
+        while (S < cap && bytes_for(S + 1) <= budget) ++S;
+        slots = (u32)S;
+    }
     pfg_server* v = new pfg_server();
     v->S = slots;
     v->t0 = std::chrono::steady_clock::now();
@@ -348,8 +384,8 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
     cudaStream_t st = s->stream;
     if (m > 0) {
         S_CUDA(cudaMemcpyAsync(v->d_adm, v->h_adm, 3 * S * 4, cudaMemcpyHostToDevice, st));
-        const u32 blocks = (u32)std::min<u64>(((u64)m * n + 255) / 256, (u64)s->sm_count * 8);
-        k_serve_clear<<<blocks, 256, 0, st>>>(s->d_state, v->d_adm, m, n);
+        const u32 bx = (u32)std::max<u64>(1, std::min<u64>(((u64)n / 2 + 255) / 256, (u64)s->sm_count * 2));
+        k_serve_clear<<<dim3(bx, m), 256, 0, st>>>(s->d_state, v->d_adm, n);
         S_CUDA(cudaGetLastError());
     }
     AdmitParams a;
@@ -417,6 +453,9 @@ extern "C" pfg_status pfg_server_step(pfg_server* v, uint32_t max_rounds, uint32
     p.ctl = s->d_ctl;
     p.delta = v->delta;
     p.mode = MODE_DELTA;
+    // learned Delta when asked for and a network is loaded; the fixed automatic Delta otherwise
+    p.policy = (v->opt.policy == PFG_POLICY_LEARNED && s->has_net) ? 1 : 0;
+    p.net = s->d_net;
     p.inst_target = v->d_target;
     p.inst_tx = v->d_tx;
     p.inst_ty = v->d_ty;
@@ -494,6 +533,7 @@ extern "C" pfg_status pfg_server_results(pfg_server* v, pfg_query_result* out, u
 }
 
 extern "C" uint32_t pfg_server_pending(const pfg_server* v) { return v ? (uint32_t)v->pending.size() : 0u; }
+extern "C" uint32_t pfg_server_slots(const pfg_server* v) { return v ? v->S : 0u; }
 extern "C" uint32_t pfg_server_in_flight(const pfg_server* v) {
     if (!v) return 0u;
     u32 k = 0;

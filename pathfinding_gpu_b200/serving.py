@@ -1,6 +1,6 @@
 """Serving A* queries with continuous batching (C ABI: pfg_server_*).
 
-    srv = GpuServer(g, slots=64)
+    srv = GpuServer(g, slots=64)     # slots=0: as many as 60 % of the free device memory holds
     qid = srv.submit(s, t)          # queued on the host
     srv.step(max_rounds=32)         # admit into free slots, run <= 32 device rounds, retire finished
     for r in srv.results(): ...     # id, src, dst, dist, slot, submit_us, admit_us, finish_us
@@ -45,7 +45,7 @@ class GpuServer:
                                             float(g.hScale), float(g.avgW), float(g.avgDeg), int(slots),
                                             C.byref(c), int(device), C.byref(h)))
         self._h = h
-        self.slots = int(slots)
+        self.slots = int(self._lib.pfg_server_slots(h))  # chosen by device memory when slots = 0
 
     def close(self):
         if getattr(self, "_h", None):

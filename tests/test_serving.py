@@ -82,3 +82,33 @@ def test_answer_all_in_query_order(oracle, road):
     with GpuServer(road, slots=5) as srv:
         got = answer_all(srv, pairs)
     assert got == [int(oracle.dijkstra(road, s)[0][t]) for s, t in pairs]
+
+
+def test_slots_by_device_memory(oracle, road):
+    # slots = 0: the server sizes itself by free device memory; answers stay exact
+    pairs = pairs_for(road, 40, 21)
+    want = oracle_dist(oracle, road, pairs)
+    with GpuServer(road, slots=0) as srv:
+        assert 1 <= srv.slots <= 2048 and srv.slots * road.n < 2 ** 32
+        ids = [srv.submit(s, t) for s, t in pairs]
+        got = {r["id"]: r["dist"] for r in srv.drain(max_rounds=8)}
+    assert [got[q] for q in ids] == want
+
+
+@pytest.mark.parametrize("schedule", ["Async", "Warp", "Rounds"])
+def test_learned_policy_and_schedules_serve_the_same_answers(oracle, road, schedule):
+    # the learned policy (when a network is loaded) and every drain change the
+    # schedule only; without a network the server falls back to the fixed Delta
+    from pathfinding_gpu_b200 import GpuOptions, Policy, Schedule
+    from pathfinding_gpu_b200 import policy as P
+    pairs = pairs_for(road, 24, 33)
+    want = oracle_dist(oracle, road, pairs)
+    opt = GpuOptions(policy=Policy.Learned, schedule=Schedule[schedule])
+    with GpuServer(road, slots=6, opt=opt) as srv:
+        ids = [srv.submit(s, t) for s, t in pairs[:12]]
+        got = {r["id"]: r["dist"] for r in srv.drain(max_rounds=8)}  # no network yet: fixed Delta
+        if P.WEIGHTS.exists():
+            srv.set_policy(P.load())
+        ids += [srv.submit(s, t) for s, t in pairs[12:]]
+        got.update({r["id"]: r["dist"] for r in srv.drain(max_rounds=8)})
+    assert [got[q] for q in ids] == want
