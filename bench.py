@@ -432,6 +432,7 @@ def extras(g):
                                               "p50": round(float(np.percentile(ts, 50)), 3),
                                               "p99": round(float(np.percentile(ts, 99)), 3)}
     # --- aggregate throughput against the batch size (roofline per launch) ---
+    from pathfinding_gpu_b200 import policy as P
     peak, _ = measured_peaks()
     sweep = {}
     Ks = (16, 32, 64, 128, 256)
@@ -453,6 +454,19 @@ def extras(g):
             sweep[str(K)] = {"ms": ms, "best": best, "gteps": round(K * g.m / ms / 1e6, 3),
                              "roofline_frac": round(b_alg / (ms * 1e-3) / 1e9 / peak, 4), "candidates_ms": cands}
     out["grid1000_batch_sweep"] = sweep
+    # the learned policy on the step's own workload (K = 64), same engine and sources
+    if P.WEIGHTS.exists():
+        with pf.GpuSolver(g, 64) as s:
+            s.set_policy(P.load())
+            fixed = HEADLINE_OPTIONS()
+            learned = replace(HEADLINE_OPTIONS(), policy=Policy.Learned)
+            tf = _median_ms(lambda: s.run_state(srcs_all[:64], fixed, copy=False)[1], 3)
+            tl = _median_ms(lambda: s.run_state(srcs_all[:64], learned, copy=False)[1], 3)
+            a = s.run_state(srcs_all[:64], fixed)[2]
+            st_l, _, b = s.run_state(srcs_all[:64], learned)
+            out["grid1000_k64_learned_vs_fixed"] = {"fixed_ms": round(tf, 3), "learned_ms": round(tl, 3),
+                                                    "speedup": round(tf / tl, 3), "buckets_learned": st_l.buckets,
+                                                    "identical_state": bool(np.array_equal(a, b))}
     # --- R-MAT scale 20: batched multi-source throughput, learned policy vs fixed automatic Delta ---
     from pathfinding_gpu_b200 import policy as P
     gr = pf.rmat(20, 16, seed=SEED)

@@ -245,6 +245,8 @@ struct RunParams {
     // Block-synchronous drain: claimed-list entries a CTA keeps beyond its pass
     // before it spills the rest to the ring while no CTA is idle (0: half a block).
     u32 spill_keep;
+    u32 idle_ns;       // block-synchronous drain: longest idle poll interval (ns; 0: 64)
+    u32 pad_idle[3];
 };
 
 // ---------------------------------------------------------------------------

@@ -951,6 +951,7 @@ __device__ __forceinline__ void async_drain(const RunParams& p, const Snap& s, L
                 bool idle = false;
                 u64 t0 = global_timer_ns();
                 u32 beat = ld_relaxed(aq + AQ_BEAT);
+                u32 nap = 32u;  // idle poll interval (ns), doubled up to p.idle_ns
                 for (u32 spin = 1;; ++spin) {
                     if ((spin & 15u) == 0u) {
                         if (vload(&c->rd.status) != DS_OK) break;
@@ -964,11 +965,15 @@ __device__ __forceinline__ void async_drain(const RunParams& p, const Snap& s, L
                             break;
                         }
                     }
-                    const u32 busy = ld_acquire(aq + AQ_BUSY);
+                    // done, then busy, then tail: a chunk's consumer takes its busy unit
+                    // before it counts the chunk done, so done == tail with busy == 0 read
+                    // in this order means no CTA held work in between
                     const u32 done = ld_acquire(aq + AQ_DONE);
+                    const u32 busy = ld_acquire(aq + AQ_BUSY);
                     const u32 t = ld_acquire(aq + AQ_TAIL);
                     const u32 hh = ld_relaxed(aq + AQ_HEAD);
                     if ((int)(t - hh) > 0) {
+                        nap = 32u;
                         const u32 avail = t - hh;
                         u32 want = (avail + G - 1u) / G;
                         want = want < 32u ? 32u : want;
@@ -992,7 +997,8 @@ __device__ __forceinline__ void async_drain(const RunParams& p, const Snap& s, L
                         atomicAdd(aq + AQ_IDLE, 1u);
                         idle = true;
                     }
-                    __nanosleep(64);
+                    __nanosleep(nap);
+                    nap = min(2u * nap, p.idle_ns ? p.idle_ns : 64u);
                 }
                 if (idle) atomicSub(aq + AQ_IDLE, 1u);
             }

@@ -423,6 +423,7 @@ void configure_drain(RunParams& p, int schedule, HubRec* hubs, u32 hub_cap, u32 
     // faster at 128-256 instances on the 1000 x 1000 grid); elsewhere half a block
     // (hub rows make spilled work pay off sooner).
     p.spill_keep = (u32)std::max(0, env_int("PFG_SPILL_KEEP", p.short_rows ? 1024 : 0));
+    p.idle_ns = (u32)std::max(0, env_int("PFG_IDLE_NS", 64));
     if (p.ring && p.warp_drain && hubs && mapping == PFG_MAP_HYBRID && max_deg > 8u * (u32)block && !p.hubs) {
         p.hubs = hubs;
         p.hub_cap = hub_cap;
