@@ -545,8 +545,10 @@ def extras(g):
     v = pf.uniform_vertices(road.n, 2 * 4000, SEED)
     qs = [(int(v[2 * i]), int(v[2 * i + 1])) for i in range(4000)]
     serving = {"graph": f"road 2048x2048, n={road.n}, m={road.m}", "bucket_drains_per_step": 8}
-    for mode in ("learned", "fixed"):
-        opt = GpuOptions(policy=Policy.Learned) if mode == "learned" else GpuOptions()
+    from pathfinding_gpu_b200 import Schedule as _Sched
+    for mode in ("learned", "fixed", "fixed_warp_drain"):
+        opt = (GpuOptions(policy=Policy.Learned) if mode == "learned" else
+               GpuOptions(schedule=_Sched.Warp) if mode == "fixed_warp_drain" else GpuOptions())
         with GpuServer(road, slots=0, opt=opt) as srv:
             if mode == "learned" and P.WEIGHTS.exists():
                 srv.set_policy(P.load())

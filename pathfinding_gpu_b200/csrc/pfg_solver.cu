@@ -559,12 +559,24 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     // mapping; its thread-mapping instantiation measured fastest.
     const int map = mode == MODE_NAIVE ? PFG_MAP_THREAD : o.mapping;
     const int block = o.block_size;
-    // Grid tier of the hybrid mapping for rows longer than 8 CTAs' worth of arcs.
-    if (s->d_hubs && (map == PFG_MAP_HYBRID || mode == MODE_NAIVE) && s->max_deg > 8u * (u32)block) {
+    // Grid tier of the hybrid mapping for rows longer than 8 CTAs' worth of arcs, claimed
+    // in chunks of 4 CTAs' worth. A single source with 1024-thread CTAs publishes rows
+    // above 4,096 arcs and claims 2,048 at a time (R-MAT-20: ~10 % faster; with 16
+    // sources the larger tier wins). PFG_HUB_BLOCKS / PFG_HUB_CHUNK_BLOCKS override both,
+    // in blocks.
+    u32 hub_min = 8u * (u32)block, hub_chunk = 4u * (u32)block;
+    if (k == 1) {
+        hub_min = std::min(hub_min, 4096u);
+        hub_chunk = std::min(hub_chunk, 2048u);
+    }
+    if (env_int("PFG_HUB_BLOCKS", 0) > 0) hub_min = (u32)env_int("PFG_HUB_BLOCKS", 0) * (u32)block;
+    if (env_int("PFG_HUB_CHUNK_BLOCKS", 0) > 0) hub_chunk = (u32)env_int("PFG_HUB_CHUNK_BLOCKS", 0) * (u32)block;
+    hub_min = std::max(hub_min, 256u);  // the records are sized for rows above 256 arcs
+    if (s->d_hubs && (map == PFG_MAP_HYBRID || mode == MODE_NAIVE) && s->max_deg > hub_min) {
         p.hubs = s->d_hubs;
         p.hub_cap = s->hub_cap;
-        p.hub_min = 8u * (u32)block;
-        p.hub_chunk = 4u * (u32)block;
+        p.hub_min = hub_min;
+        p.hub_chunk = hub_chunk;
         p.aq = s->d_aq;
     }
     configure_drain(p, o.schedule, s->d_hubs, s->hub_cap, s->max_deg, s->d_aq, map, block);
