@@ -114,24 +114,30 @@ def infer(params, X) -> np.ndarray:
     return out
 
 
-def run_traced(solver: GpuSolver, src: int, opt: GpuOptions, cap: int = 4096):
-    """One traced Delta-stepping run: (stats, ms, trace rows [r, 16])."""
+def _sources(src) -> List[int]:
+    """One source, or a batch of sources run as one multi-source launch."""
+    return [int(src)] if isinstance(src, (int, np.integer)) else [int(x) for x in src]
+
+
+def run_traced(solver: GpuSolver, src, opt: GpuOptions, cap: int = 4096):
+    """One traced Delta-stepping run of one source or a batch: (stats, ms, trace rows [r, 16])."""
     lib = N.load()
     from .solver import GpuStats
-    srcs = np.ascontiguousarray([src], np.uint32)
+    srcs = np.ascontiguousarray(_sources(src), np.uint32)
     c = opt.to_c()
     st = N.PfgStats()
     buf = np.empty((cap, TRACE_W), np.float32)
     rows = C.c_uint32()
     ms = C.c_float()
-    N.check(lib.pfg_run_traced(solver.handle, N.ptr(srcs, N.u32), 1, C.byref(c), C.byref(st),
+    N.check(lib.pfg_run_traced(solver.handle, N.ptr(srcs, N.u32), len(srcs), C.byref(c), C.byref(st),
                                N.ptr(buf, N.f32), cap, C.byref(rows), C.byref(ms)))
     return GpuStats.from_c(st), float(ms.value), buf[: rows.value].copy()
 
 
 def collect(solver: GpuSolver, sources: Iterable[int], reps: int = 3, rows_per_run: int = 96,
             base: Optional[GpuOptions] = None, seed: int = 0):
-    """Traces and soft targets from fixed-Delta sweeps over CLASSES.
+    """Traces and soft targets from fixed-Delta sweeps over CLASSES (each element of
+    `sources` is one source or a batch of sources run as one multi-source launch).
 
     Each source's sweep is normalised by its fastest multiplier and the curves of
     all sources of the graph are averaged; every trace row of the graph gets the
@@ -146,11 +152,11 @@ def collect(solver: GpuSolver, sources: Iterable[int], reps: int = 3, rows_per_r
         for sched, mult in CLASSES:
             d = max(1, int(auto * mult))  # the kernel truncates the same product
             o = GpuOptions(**{**base.__dict__, "delta": d, "policy": Policy.Fixed, "schedule": sched})
-            solver.run_state([src], o, copy=False)  # warm
+            solver.run_state(_sources(src), o, copy=False)  # warm
             ts = []
             tr = None
             for r in range(reps):
-                st, ms, rows = run_traced(solver, int(src), o)
+                st, ms, rows = run_traced(solver, src, o)
                 ts.append(ms)
                 tr = rows
             times.append(statistics.median(ts))
@@ -158,7 +164,9 @@ def collect(solver: GpuSolver, sources: Iterable[int], reps: int = 3, rows_per_r
                 tr = tr[np.sort(rng.choice(len(tr), rows_per_run, replace=False))]
             traces.append(tr)
         curves.append(np.asarray(times) / min(times))
-        table.append({"src": int(src), "times_ms": [round(t, 4) for t in times],
+        srcs = _sources(src)
+        table.append({"src": srcs[0] if len(srcs) == 1 else f"batch of {len(srcs)} from {srcs[0]}",
+                      "times_ms": [round(t, 4) for t in times],
                       "best": class_name(int(np.argmin(times)))})
     mean_curve = np.mean(curves, axis=0)
     y = soft_targets(mean_curve)

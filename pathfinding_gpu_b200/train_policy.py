@@ -4,7 +4,8 @@
 
 1. Traces: for every (graph, source) of the training families (R-MAT scales 19-20
    with two edge factors and two weight ranges, seeds other than the evaluation
-   graph's; grids of 256-768 per side; a road-like grid), fixed-Delta
+   graph's; grids of 256-768 per side; a road-like grid; batches of 32-64 sources on grids and
+   the road-like grid, run as one multi-source launch), fixed-Delta
    runs of each class of policy.CLASSES (schedule x multiplier) are timed and
    traced.
 2. Training: full-batch Adam with the hand-written kernels of pfg_policy.cu.
@@ -38,16 +39,23 @@ TRAIN_FAMILIES = [
     ("grid_512", lambda: G.grid(512, 512, 22)),
     ("grid_768", lambda: G.grid(768, 768, 23)),
     ("road_512", lambda: G.road(512, seed=24)),
+    # batches of sources sharing one bucket sequence (multi-source launches)
+    ("grid_512_k64", lambda: G.grid(512, 512, 25), 64),
+    ("grid_768_k32", lambda: G.grid(768, 768, 26), 32),
+    ("grid_768_k64", lambda: G.grid(768, 768, 27), 64),
+    ("road_512_k64", lambda: G.road(512, seed=28), 64),
 ]
 EVAL = [
     ("rmat_s20_ef16_seed2026", lambda: G.rmat(20, 16, seed=2026)),
     ("grid_1000_seed2026", lambda: G.grid(1000, 1000, 2026)),
+    ("grid_1000_seed2026_k64", lambda: G.grid(1000, 1000, 2026), 64),
 ]
 
 
 def timed(solver, src, opt, reps=5):
-    solver.run_state([src], opt, copy=False)
-    return statistics.median(solver.run_state([src], opt, copy=False)[1] for _ in range(reps))
+    srcs = P._sources(src)
+    solver.run_state(srcs, opt, copy=False)
+    return statistics.median(solver.run_state(srcs, opt, copy=False)[1] for _ in range(reps))
 
 
 def main(argv=None):
@@ -62,10 +70,14 @@ def main(argv=None):
     report = {"families": {}, "eval": {}}
     Xs, Ys = [], []
     t0 = time.time()
-    for name, make in TRAIN_FAMILIES:
+    for fam in TRAIN_FAMILIES:
+        name, make, k = fam if len(fam) == 3 else (*fam, 1)
         g = make()
-        with GpuSolver(g, 1) as s:
-            srcs = G.pick_sources(g, args.sources, 7).tolist()
+        with GpuSolver(g, k) as s:
+            if k == 1:
+                srcs = G.pick_sources(g, args.sources, 7).tolist()
+            else:  # two batches of k sources
+                srcs = [tuple(G.uniform_vertices(g.n, k, 7 + b).tolist()) for b in range(2)]
             X, Y, table, curve = P.collect(s, srcs, base=base, reps=5)
         Xs.append(X)
         Ys.append(Y)
@@ -82,21 +94,22 @@ def main(argv=None):
     print(f"[train] rows {len(X)} loss {losses[0]:.4f} -> {losses[-1]:.4f}, argmax agreement {acc:.3f}", flush=True)
     P.save(params, Path(args.out), {"steps": args.steps, "lr": args.lr, "rows": len(X)})
 
-    for name, make in EVAL:
+    for fam in EVAL:
+        name, make, k = fam if len(fam) == 3 else (*fam, 1)
         g = make()
-        with GpuSolver(g, 1) as s:
+        with GpuSolver(g, k) as s:
             s.set_policy(params)
-            srcs = G.pick_sources(g, 3, 99).tolist()
+            srcs = G.pick_sources(g, 3, 99).tolist() if k == 1 else [tuple(G.uniform_vertices(g.n, k, 2026).tolist())]
             rows = []
             for src in srcs:
                 fixed = GpuOptions(**{**base.__dict__})
                 learned = GpuOptions(**{**base.__dict__, "policy": Policy.Learned})
                 tf = timed(s, src, fixed)
                 tl = timed(s, src, learned)
-                _, _, a = s.run_state([src], fixed)
-                sl, _, b = s.run_state([src], learned)
+                _, _, a = s.run_state(P._sources(src), fixed)
+                sl, _, b = s.run_state(P._sources(src), learned)
                 _, _, tr = P.run_traced(s, src, learned)
-                rows.append({"src": src, "fixed_ms": round(tf, 4), "learned_ms": round(tl, 4),
+                rows.append({"src": src if k == 1 else f"batch of {k}", "fixed_ms": round(tf, 4), "learned_ms": round(tl, 4),
                              "speedup": round(tf / tl, 3), "bit_exact": bool(np.array_equal(a, b)),
                              "learned_buckets": sl.buckets,
                              "learned_deltas": [int(x) for x in tr[:, P.IN + 1]],
