@@ -246,7 +246,11 @@ struct RunParams {
     // before it spills the rest to the ring while no CTA is idle (0: half a block).
     u32 spill_keep;
     u32 idle_ns;       // block-synchronous drain: longest idle poll interval (ns; 0: 64)
-    u32 pad_idle[3];
+    // 1: entries of asynchronous buckets are relaxed with the distance they carry, without
+    // reading the state first (about a third of the entries are stale and relaxed anyway;
+    // set for single-source runs on graphs of short rows, which are latency-bound)
+    u32 trust_entries;
+    u32 pad_idle[2];
 };
 
 // ---------------------------------------------------------------------------

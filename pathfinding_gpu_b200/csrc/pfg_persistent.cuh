@@ -523,8 +523,15 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
         r0 = __ldg(p.prow + rb + u);
         r1 = __ldg(p.prow + rb + u + 1);
     }
-    du = st_dist(ld_state(p.state + gi));
-    if (want != INF32 && du != want) return false;
+    if (want != INF32 && p.trust_entries) {
+        // single-source runs on short rows: the entry's own distance, without the state
+        // read - a hop is one round trip instead of two, and a stale entry (its vertex
+        // improved since) only relaxes upper bounds that the newer entry's values override
+        du = want;
+    } else {
+        du = st_dist(ld_state(p.state + gi));
+        if (want != INF32 && du != want) return false;  // stale: the newer entry relaxes it
+    }
     bool act = du != INF32;
     u64 key = du;
     if constexpr (ASTAR) {
