@@ -71,9 +71,19 @@ enum pfg_policy_kind { PFG_POLICY_FIXED = 0, PFG_POLICY_LEARNED = 1 };
  *         block barrier between batches (Hybrid mapping only; other mappings
  *         run ASYNC). It sustains more throughput on large batches (hundreds of
  *         instances), ASYNC has the lower latency on small ones.
- * AUTO:   ASYNC for Delta-stepping, ROUNDS for Naive and Frontier. */
+ * INSTANCE: ASYNC with a window per instance of a multi-source run: each
+ *         instance advances to its next bucket as soon as its own entries are
+ *         drained, with no grid barrier between buckets; the automatic Delta
+ *         (delta = 0) is 4 x the single-source rule under it. Applies to solver
+ *         runs of 2..256 sources with the Hybrid mapping, the fixed Delta
+ *         policy and block_size >= 64 when Delta >= the largest weight (every
+ *         arc light) and no row has more than 8 x block_size arcs; elsewhere it
+ *         runs as ASYNC.
+ * AUTO:   INSTANCE where it applies to a batch of 128 or more sources
+ *         (environment PFG_INST_WINDOWS: that threshold, 0 = never), else ASYNC
+ *         for Delta-stepping; ROUNDS for Naive and Frontier. */
 enum pfg_schedule { PFG_SCHEDULE_AUTO = 0, PFG_SCHEDULE_ROUNDS = 1, PFG_SCHEDULE_ASYNC = 2,
-                    PFG_SCHEDULE_WARP = 3 };
+                    PFG_SCHEDULE_WARP = 3, PFG_SCHEDULE_INSTANCE = 4 };
 
 /* Mirrors GpuOptions (reference: include/gpu_sssp.h:42-52) plus `policy`. */
 typedef struct pfg_options {

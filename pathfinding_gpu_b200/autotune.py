@@ -19,7 +19,9 @@ from typing import Callable, Dict, Optional, Tuple
 from .solver import AtomicMode, Compaction, GpuAlgo, GpuOptions, Mapping, Policy, Schedule
 
 LAUNCH_SHAPES = [(256, 4), (512, 2), (1024, 1)]       # (threads per CTA, CTAs per SM)
-SCHEDULES = [Schedule.Auto, Schedule.Warp]           # asynchronous drains: CTA passes / warp workers
+# asynchronous drains: automatic (a window per instance where that applies), one shared
+# window with CTA passes, warp workers
+SCHEDULES = [Schedule.Auto, Schedule.Async, Schedule.Warp]
 ATOMICS = [AtomicMode.MinRBA, AtomicMode.MinNoCheck]
 EAGER = [0, 2, 4, 8]
 DELTA_MULT = [0.25, 0.5, 1.0, 2.0, 4.0, 16.0]

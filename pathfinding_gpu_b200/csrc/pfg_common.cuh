@@ -57,6 +57,17 @@ enum RingCounter : u32 { AQ_HEAD = 0, AQ_TAIL = 32, AQ_DONE = 64, AQ_BUSY = 96, 
 // RING_FREE marks a free slot (no entry has index 2^32 - 1 and distance INF).
 constexpr unsigned long long RING_FREE = ~0ull;
 
+// Independent bucket windows (RunParams::iw): a ring entry whose index has
+// IW_FAR_BIT set is an item of its instance's far pile, queued when the
+// instance's window advanced; its high half is the start of that window.
+constexpr u32 IW_FAR_BIT = 0x80000000u;
+constexpr u32 IW_MAX_INST = 256;  // instances of one run that may use independent windows
+enum IwMisc : u32 { IW_ACTIVE = 0, IW_MAXEP = 1, IW_ADVANCES = 2, IW_MISC_WORDS = 32 };
+// Device words of the independent-window block for k instances: window words
+// (u64 [k]), pending units [k], far-pile counts [2k], far-pile minima [2k],
+// then IW_MISC_WORDS counters.
+__host__ __device__ constexpr unsigned long long iw_words(unsigned k) { return 7ull * k + IW_MISC_WORDS + 2ull; }
+
 // Grid tier of the hybrid mapping: an item whose selected arcs exceed
 // RunParams::hub_min is published as a hub record, and any CTA claims chunks
 // of hub_chunk arcs of it (aq[AQ_HUBS] counts the records of the current
@@ -250,7 +261,20 @@ struct RunParams {
     // reading the state first (about a third of the entries are stale and relaxed anyway;
     // set for single-source runs on graphs of short rows, which are latency-bound)
     u32 trust_entries;
-    u32 pad_idle[2];
+    // Independent bucket windows (iw = 1; multi-source Delta-stepping on graphs without hub
+    // rows and with every arc light): instance i advances its own window [lo, hi) as soon as
+    // its own entries are drained, so no grid barrier separates buckets and CTAs whose
+    // instance finished a bucket work on other instances' buckets instead of waiting for the
+    // slowest one. iw_win[i] = hi << 32 | far epoch << 1 | far pile in use; iw_pend[i] counts
+    // the instance's queued entries plus one unit per CTA holding some of them in shared
+    // memory, so it is zero exactly when the instance's window is drained; its far piles are
+    // farq[b] + i * n with iw_fcnt[b * k + i] items and smallest key iw_fmin[b * k + i].
+    u32 iw;
+    unsigned long long* iw_win;
+    u32* iw_pend;
+    u32* iw_fcnt;
+    u32* iw_fmin;
+    u32* iw_misc;
 };
 
 // ---------------------------------------------------------------------------

@@ -27,7 +27,7 @@ pfg_options default_options();
 void sanitize_options(pfg_options& o);
 
 // Launch shape: CTAs per SM for the persistent kernel.
-int blocks_per_sm_for(const pfg_options& o, bool astar, int map);
+int blocks_per_sm_for(const pfg_options& o, bool astar, int map, bool iw = false, u32 k = 0);
 
 // Eager sub-rounds per grid round of the hybrid mapping when the caller leaves
 // the choice to the engine (pfg_options::eager < 0), and the average degree
@@ -89,6 +89,7 @@ struct pfg_solver {
     unsigned long long* d_ring = nullptr;  // ring queue of asynchronous buckets [ring_mask + 1], RING_FREE when idle
     u32 ring_mask = 0;
     u32* d_aq = nullptr;        // ring counters [AQ_WORDS]
+    u32* d_iw = nullptr;        // independent-window block [iw_words(K)] (K <= IW_MAX_INST)
     pfg::HubRec* d_hubs = nullptr;  // hub records of the grid tier [hub_cap]
     u32 hub_cap = 0;
     u32* d_srcs = nullptr;

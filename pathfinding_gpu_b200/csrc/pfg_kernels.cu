@@ -58,8 +58,9 @@ static cudaError_t allow_coop_smem(bool astar, int am, int map, bool wd) {
     const bool w = wd && map == 2;
     const unsigned bit = 1u << ((w ? 18 : 0) + (astar ? 9 : 0) + 3 * am + map);
     if (dev < 64 && (done[dev].load() & bit)) return cudaSuccess;
+    // (room for the independent-window arrays of the largest batch that uses them)
     e = cudaFuncSetAttribute(kernel_for(astar, am, map, w), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)coop_bytes(MAX_BS));
+                             (int)(iw_smem_offset(MAX_BS) + iw_smem_bytes(IW_MAX_INST)));
     if (e == cudaSuccess && dev < 64) done[dev].fetch_or(bit);
     return e;
 }
@@ -79,7 +80,8 @@ cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, i
     const void* k = kernel_for(astar, am, map, wd);
     const cudaError_t ea = allow_coop_smem(astar, am, map, wd);
     if (ea != cudaSuccess) return ea;
-    cfg.dynamicSmemBytes = coop_bytes((u32)block);
+    if (p.iw && (astar || map != 2 || wd || p.k > IW_MAX_INST)) return cudaErrorInvalidValue;
+    cfg.dynamicSmemBytes = p.iw ? iw_smem_offset((u32)block) + iw_smem_bytes(p.k) : coop_bytes((u32)block);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -90,13 +92,15 @@ cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, i
     return cudaLaunchKernelExC(&cfg, k, args);
 }
 
-int persistent_blocks_per_sm(bool astar, int am, int map, int block, bool wd) {
+// iw_k > 0: with the independent-window arrays of a run of iw_k instances.
+int persistent_blocks_per_sm(bool astar, int am, int map, int block, bool wd, u32 iw_k) {
     int nb = 0;
     if (am < 0 || am > 2) am = 0;
     if (map < 0 || map > 2) map = 2;
     const void* k = kernel_for(astar, am, map, wd);
+    const size_t dyn = iw_k ? iw_smem_offset((u32)block) + iw_smem_bytes(iw_k) : coop_bytes((u32)block);
     if (allow_coop_smem(astar, am, map, wd) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block, coop_bytes((u32)block)) != cudaSuccess) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block, dyn) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }

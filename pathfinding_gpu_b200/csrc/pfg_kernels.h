@@ -14,7 +14,7 @@ cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, i
                               int grid, cudaStream_t st);
 // Largest number of co-resident CTAs per SM for that instantiation (0 on error);
 // wd: the warp-drain instantiation (hybrid mapping).
-int persistent_blocks_per_sm(bool astar, int am, int map, int block, bool wd = false);
+int persistent_blocks_per_sm(bool astar, int am, int map, int block, bool wd = false, u32 iw_k = 0);
 
 // Builds the padded interleaved adjacency adj[prow[u] ..] from a plain CSR.
 cudaError_t launch_build_adj(const uint32_t* row, const uint32_t* col, const uint32_t* w,

@@ -122,6 +122,33 @@ __device__ __forceinline__ unsigned long long* wq_slots(Coop& cs) {
 // u64 ub[block], u32 off[block + 1], eb[block], u[block], du[block], ib[block], inst[block].
 __host__ __device__ constexpr size_t coop_bytes(u32 block) { return sizeof(Coop) + (size_t)block * 32u + 4u; }
 
+// Independent bucket windows (RunParams::iw): per-CTA arrays over the k
+// instances, after the per-thread arrays: the window word of each instance the
+// CTA holds, the entries of it the CTA holds (claimed list and the current
+// pass), the entries of it finished in the current pass, the CTA's hold on it
+// (IW_FREE / IW_HELD / IW_RELEASING), the instances whose windows the CTA
+// advances next, and the holds its service warp releases during the next pass.
+__host__ __device__ constexpr size_t iw_smem_offset(u32 block) { return (coop_bytes(block) + 15u) & ~(size_t)15u; }
+__host__ __device__ constexpr size_t iw_smem_bytes(u32 k) { return (size_t)k * 28u + 16u; }
+enum IwHold : u32 { IW_FREE = 0, IW_HELD = 1, IW_RELEASING = 2 };
+struct IwSh {
+    unsigned long long* win;
+    u32 *lc, *fin, *held, *adv, *rel, *adv_n, *rel_n;
+};
+__device__ __forceinline__ IwSh iw_sh(const Coop* cs, u32 k) {
+    unsigned char* b = (unsigned char*)cs + iw_smem_offset(blockDim.x);
+    IwSh r;
+    r.win = reinterpret_cast<unsigned long long*>(b);
+    r.lc = reinterpret_cast<u32*>(b + 8u * k);
+    r.fin = r.lc + k;
+    r.held = r.fin + k;
+    r.adv = r.held + k;
+    r.rel = r.adv + k;
+    r.adv_n = r.rel + k;
+    r.rel_n = r.adv_n + 1;
+    return r;
+}
+
 // ---------------------------------------------------------------------------
 // Block-wide exclusive scan (warp shuffles + one pass over warp totals).
 // ---------------------------------------------------------------------------
@@ -306,10 +333,15 @@ __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, 
         if (slot - cl->cl_head < CL_CAP) {
             cl->cl[slot & (CL_CAP - 1u)] = gv;
             cl->cl_d[slot & (CL_CAP - 1u)] = nd;
+            if (p.iw) atomicAdd(iw_sh(cl, p.k).lc + inst, 1u);  // held by this CTA
             return;
         }
     }
     if (s.async_bkt) {
+        if (p.iw) {  // a pending unit of its own, counted before the entry can be taken
+            atomicAdd(p.iw_pend + inst, 1u);
+            __threadfence();
+        }
         if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, ((unsigned long long)nd << 32) | gv, p.timeout_ns))
             flag_timeout(c, WS_RING_PUSH);
         return;
@@ -318,10 +350,31 @@ __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, 
     queue_push(p.nearq[out], &c->cnt[C_NEAR0 + out], gv);
 }
 
+// Independent windows: gi (of instance inst) was improved to `key`, at or
+// beyond its instance's window end. The far pile in use and its epoch come
+// with the window word w; the pile's minimum is lowered for every such
+// improvement, and the vertex is queued once per epoch (so a pile never holds
+// more than n items).
+__device__ __forceinline__ void iw_far_push(const RunParams& p, u32 gi, u32 inst, u32 key, u64 w, Local& L) {
+    const u32 fs = (u32)w & 1u, fe = (u32)w >> 1;
+    atomicMin(p.iw_fmin + fs * p.k + inst, key);
+    if (claim_stamp(p.far_stamp, gi, fe)) {
+        const u32 pos = atomicAdd(p.iw_fcnt + fs * p.k + inst, 1u);
+        if (pos < p.n)
+            p.farq[fs][(size_t)inst * p.n + pos] = gi;
+        else  // (one push per vertex and epoch: cannot happen)
+            atomicCAS(&p.ctl->rd.status, (u32)DS_OK, (u32)DS_NOT_CONVERGED);
+        L.pushes++;
+    }
+}
+
 // After gv's distance was lowered to a value of key `key`: flag it (prefix-scan
-// compaction) or claim it for the window / the far pile and queue it.
+// compaction) or claim it for the window / the far pile and queue it. ub: the
+// A* pruning bound, or (SSSP) the window word of the item's instance under
+// independent windows (~0 otherwise).
+template <bool ASTAR>
 __device__ __forceinline__ void after_improve(const RunParams& p, const Snap& s, u32 gv, u64 key, u32 nd,
-                                              u32 inst, Local& L, Coop* cl) {
+                                              u32 inst, u64 ub, Local& L, Coop* cl) {
     L.updates++;
     if (p.mode == MODE_NAIVE) {  // Bellman-Ford sweep: the head is active in the next sweep
         atomicOr(p.naive_mask[s.naive_in ^ 1u] + (gv >> 5), 1u << (gv & 31u));
@@ -333,7 +386,16 @@ __device__ __forceinline__ void after_improve(const RunParams& p, const Snap& s,
         L.pushes++;
         return;
     }
-    const bool near = key < s.hi;
+    // (independent windows: the shared window is unbounded and the instance's
+    // window end is the high half of ub; SSSP runs otherwise pass ub = ~0)
+    const bool near = key < s.hi && (ASTAR || key < (ub >> 32));
+    if (!ASTAR && p.iw) {
+        if (near)
+            push_claimed(p, s, gv, nd, true, inst, L, cl);
+        else
+            iw_far_push(p, gv, inst, (u32)key, ub, L);
+        return;
+    }
     if (!near) L.fmin = key < L.fmin ? key : L.fmin;
     if (near && s.async_bkt) {
         // Asynchronous bucket: no claim. Every strict improvement queues an
@@ -373,7 +435,7 @@ __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32
     if (!arc_candidate<ASTAR>(p, du, ub, inst, v, w, L, nd, key)) return;
     const u32 gv = ib + v;
     if (!relax_state<AM>(p.state + gv, (u32)nd, u, L.atomics)) return;
-    after_improve(p, s, gv, key, (u32)nd, inst, L, cl);
+    after_improve<ASTAR>(p, s, gv, key, (u32)nd, inst, ub, L, cl);
 }
 
 // Two arcs of one lane relaxed together: both state updates are issued before
@@ -407,8 +469,8 @@ __device__ __forceinline__ void relax_arc_pair(const RunParams& p, const Snap& s
         ia = ta && st_dist(oa) > (u32)nda;
         ibt = tb && st_dist(ob) > (u32)ndb;
     }
-    if (ia) after_improve(p, s, gva, keya, (u32)nda, insta, L, cl);
-    if (ibt) after_improve(p, s, gvb, keyb, (u32)ndb, instb, L, cl);
+    if (ia) after_improve<ASTAR>(p, s, gva, keya, (u32)nda, insta, uba, L, cl);
+    if (ibt) after_improve<ASTAR>(p, s, gvb, keyb, (u32)ndb, instb, ubb, L, cl);
 }
 
 // Thread tier: one thread walks its own arcs [eb, ee) with 128-bit loads
@@ -468,7 +530,7 @@ __device__ __forceinline__ void relax4(const RunParams& p, const Snap& s, u32 u,
         if (go[j]) {
             u64 key = nd[j];
             if constexpr (ASTAR) key = astar_key(p, inst, hv[j], nd[j]);
-            after_improve(p, s, ib + hv[j], key, nd[j], inst, L, cl);
+            after_improve<ASTAR>(p, s, ib + hv[j], key, nd[j], inst, ub, L, cl);
         }
     }
 }
@@ -679,7 +741,7 @@ __device__ __forceinline__ void relax_items_warp(const RunParams& p, const Snap&
         const u32 bib = __shfl_sync(FULL, ib, lob), binst = __shfl_sync(FULL, inst, lob);
         const u32 beb = __shfl_sync(FULL, eb, lob) + (jb - __shfl_sync(FULL, off, lob));
         u64 aub = ~0ull, bub = ~0ull;
-        if constexpr (ASTAR) {
+        if (ASTAR || p.iw) {  // (warp-uniform)
             aub = __shfl_sync(FULL, ub, loa);
             bub = __shfl_sync(FULL, ub, lob);
         }
@@ -702,7 +764,7 @@ __device__ __forceinline__ void relax_items_warp(const RunParams& p, const Snap&
         const u32 wib = __shfl_sync(FULL, ib, lo), winst = __shfl_sync(FULL, inst, lo);
         const u32 web = __shfl_sync(FULL, eb, lo), woff = __shfl_sync(FULL, off, lo);
         u64 wub = ~0ull;
-        if constexpr (ASTAR) wub = __shfl_sync(FULL, ub, lo);
+        if (ASTAR || p.iw) wub = __shfl_sync(FULL, ub, lo);
         if (j < total) {
             const uint2 a = __ldg(p.adj + web + (j - woff));
             relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, winst, a.x, a.y, L, cl);
@@ -1123,6 +1185,471 @@ __device__ __forceinline__ void async_drain(const RunParams& p, const Snap& s, L
                 }
                 atomicAdd(aq + AQ_DONE, n);
             }
+        }
+    }
+    if (threadIdx.x == 0) {
+        cs.cl_n = 0u;
+        cs.cl_head = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Independent bucket windows (RunParams::iw = 1): one drain for the whole run.
+//
+// Every instance i has its own window [lo_i, hi_i). An improvement below hi_i
+// queues an entry (claimed list or ring) as in an asynchronous bucket; one at
+// or beyond it goes to the instance's far pile. iw_pend[i] counts the
+// instance's entries in the ring plus one unit per CTA holding entries of it in
+// its claimed list or its current pass, so it reaches zero exactly when nothing
+// of the window is left anywhere: the CTA that releases the last unit advances
+// the window (the next aligned window above the pile's smallest key, as a
+// bucket advance does) and queues the pile's items in the ring, marked with
+// IW_FAR_BIT and the old window end, for any CTA to classify and relax. An
+// instance whose far pile is empty at its advance is finished; the drain ends
+// when every instance is.
+//
+// Pending units: a ring entry carries one; the first entry of an instance that
+// a CTA takes while holding none of it turns that unit into the CTA's hold, the
+// others give theirs back; an entry pushed to the claimed list is covered by
+// the hold, one that overflows to the ring gets its own unit before it is
+// written, and so do entries spilled to the ring, before any of them is
+// written. A CTA whose pass leaves it with no entry of an instance marks its
+// hold IW_RELEASING; its service warp (warp 0, which relaxes nothing) releases
+// it during the next pass, after a fence, so the far pushes and state updates
+// of the CTA's passes are visible to whoever advances the window, and the fence
+// and the returning atomic stay off the other warps' path. A ring entry of the
+// instance taken before that cancels the release instead (the hold goes on);
+// one compare-and-swap on the hold word decides which of the two happens. A
+// CTA about to wait for work releases its marked holds first.
+//
+// Results do not depend on the order: every strict improvement is relaxed (near
+// entries) or kept (far pile) until its window comes, so the final state is the
+// same unique fixed point as with a shared window.
+// ---------------------------------------------------------------------------
+
+// Per warp: arr[key] += delta for each lane with v, one atomic per distinct
+// key (every lane of the warp calls it).
+__device__ __forceinline__ void warp_add_keyed(u32* arr, u32 key, int delta, bool v) {
+    const unsigned vm = __ballot_sync(FULL, v);
+    if (!v) return;
+    const unsigned m = __match_any_sync(vm, key);
+    if ((threadIdx.x & 31u) == (u32)(__ffs(m) - 1)) atomicAdd(arr + key, (u32)(delta * __popc(m)));
+}
+
+// Ring entries taken by this pass become the CTA's (every lane of the warp calls
+// it; v: this lane took a ring entry of instance inst, whose window word is w).
+__device__ __forceinline__ void iw_take_ring(const RunParams& p, const IwSh& sh, u32 inst, u64 w, bool v) {
+    const unsigned vm = __ballot_sync(FULL, v);
+    if (!v) return;
+    const unsigned m = __match_any_sync(vm, inst);
+    if ((threadIdx.x & 31u) == (u32)(__ffs(m) - 1)) {
+        const u32 cnt = __popc(m);
+        u32 give = cnt;
+        if (atomicAdd(sh.lc + inst, cnt) == 0u) {
+            // the CTA held no entry of the instance: a hold being released goes on,
+            // otherwise one of the entries' units becomes the CTA's hold
+            if (atomicCAS(sh.held + inst, (u32)IW_RELEASING, (u32)IW_HELD) != (u32)IW_RELEASING) {
+                sh.held[inst] = IW_HELD;
+                sh.win[inst] = w;
+                give = cnt - 1u;
+            }
+        }
+        if (give) atomicSub(p.iw_pend + inst, give);
+    }
+}
+
+// Releases the hold on instance j unless a ring take cancelled it; lists j for
+// an advance when that was the instance's last unit. fenced: the caller issued
+// the fence that makes the CTA's earlier writes visible first.
+__device__ __forceinline__ void iw_release(const RunParams& p, const IwSh& sh, u32 j, u32 K, Ctl* c) {
+    if (atomicCAS(sh.held + j, (u32)IW_RELEASING, (u32)IW_FREE) != (u32)IW_RELEASING) return;
+    if (atomicSub(p.iw_pend + j, 1u) == 1u) {
+        // (an instance is listed at most once: its count stays zero until its advance)
+        const u32 a = atomicAdd(sh.adv_n, 1u);
+        if (a < K)
+            sh.adv[a] = j;
+        else
+            atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_NOT_CONVERGED);
+    }
+}
+
+// Classifies an entry of instance inst (state index gi, carried value cv, window
+// word w, state word sw read with it): a near entry (cv = the distance it was
+// queued with) is stale when the vertex has been improved since; a far-pile item
+// (far, cv = the window start of the advance that queued it) is relaxed when its
+// distance lies in [cv, window end), kept far beyond it, and dropped below it
+// (its window relaxed that value already). On true, [eb, ee) are the vertex's
+// arcs (every arc is light under independent windows).
+__device__ __forceinline__ bool take_iw(const RunParams& p, u32 gi, u32 inst, bool far, u32 cv, u64 w, u64 sw,
+                                        Local& L, u32& u, u32& ib, u32& du, u32& eb, u32& ee) {
+    ib = inst * p.n;
+    u = gi - ib;
+    u32 r0, r1;
+    if (p.row_stride) {
+        r0 = ROW_ALIGN * u;
+        r1 = r0 + ROW_ALIGN;
+    } else {
+        r0 = __ldg(p.prow + u);
+        r1 = __ldg(p.prow + u + 1);
+    }
+    du = st_dist(sw);
+    if (!far) {
+        if (du != cv) return false;  // stale: the newer entry relaxes it
+    } else {
+        if (du == INF32 || du < cv) return false;
+        if (du >= (u32)(w >> 32)) {
+            iw_far_push(p, gi, inst, du, w, L);
+            return false;
+        }
+    }
+    eb = r0;
+    ee = r1;
+    return ee > eb;
+}
+
+// Advances the window of instance j, whose pending count this CTA brought to
+// zero: nothing of its window is left, so its far pile is complete. Called by
+// every thread of the CTA.
+static __device__ __noinline__ void iw_advance(const RunParams& p, const Snap& s, u32 j) {
+    __shared__ u32 s_c, s_base, s_lo, s_fs;
+    if (threadIdx.x == 0) {
+        __threadfence();  // the releases that led here, before the pile is read
+        const u32 k = p.k;
+        const unsigned long long w = ld_relaxed64(p.iw_win + j);
+        const u32 fs = (u32)w & 1u, fe = (u32)w >> 1, lo = (u32)(w >> 32);
+        const u32 c = ld_relaxed(p.iw_fcnt + fs * k + j);
+        const u32 est = ld_relaxed(p.iw_fmin + fs * k + j);
+        u32 cnt = 0u;
+        if (c == 0u || est == INF32) {
+            atomicSub(p.iw_misc + IW_ACTIVE, 1u);  // nothing left beyond the window: finished
+        } else {
+            const u64 d = s.delta ? s.delta : 1u;
+            u64 hi = ((u64)est / d + 1ull) * d;  // aligned, as a fixed-Delta bucket advance
+            if (hi > 0xFFFFFFFFull) hi = 0xFFFFFFFFull;
+            const u32 nfs = fs ^ 1u, nfe = fe + 1u;
+            p.iw_fcnt[nfs * k + j] = 0u;
+            p.iw_fmin[nfs * k + j] = INF32;
+            p.iw_win[j] = (hi << 32) | ((unsigned long long)nfe << 1) | nfs;
+            atomicAdd(p.iw_pend + j, c);  // one unit per queued item
+            atomicMax(p.iw_misc + IW_MAXEP, nfe);
+            atomicAdd(p.iw_misc + IW_ADVANCES, 1u);
+            __threadfence();  // the window and the pending count before any item can be taken
+            s_base = atomicAdd(p.aq + AQ_TAIL, c);
+            cnt = c;
+        }
+        s_c = cnt;
+        s_lo = lo;
+        s_fs = fs;
+    }
+    __syncthreads();
+    const u32 c = s_c;
+    if (c) {
+        const u32* pile = p.farq[s_fs] + (size_t)j * p.n;
+        const unsigned long long hw = (unsigned long long)s_lo << 32;
+        const u32 base = s_base, BS = blockDim.x;
+        constexpr int U = 4;  // items per thread in flight: all loads, then all swaps
+        for (u32 i0 = 0; i0 < c; i0 += U * BS) {
+            unsigned long long ent[U];
+            bool ok[U];
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                const u32 i = i0 + q * BS + threadIdx.x;
+                ent[q] = i < c ? hw | (unsigned long long)(__ldcg(pile + i) | IW_FAR_BIT) : RING_FREE;
+            }
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                const u32 i = i0 + q * BS + threadIdx.x;
+                ok[q] = i >= c || atomicCAS(p.ring + ((base + i) & p.ring_mask), RING_FREE, ent[q]) == RING_FREE;
+            }
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                if (ok[q]) continue;
+                // the slot's previous entry is not taken yet (bounded wait)
+                unsigned long long* slot = p.ring + ((base + i0 + q * BS + threadIdx.x) & p.ring_mask);
+                const u64 t0 = global_timer_ns();
+                while (atomicCAS(slot, RING_FREE, ent[q]) != RING_FREE) {
+                    if (global_timer_ns() - t0 > p.timeout_ns) {
+                        flag_timeout(p.ctl, WS_SPILL_SLOT);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Starts a run under independent windows (transition thread, at INIT): every
+// instance's first window [0, Delta), one pending unit each, the sources queued
+// in the ring with distance 0.
+__device__ __forceinline__ void enter_iw(const RunParams& p, Ctl& sc, Rd& r) {
+    const u32 k = p.k;
+    const u64 hi = r.delta ? (u64)r.delta : 1ull;
+    const u32 fe = r.far_epoch;
+    for (u32 i = 0; i < k; ++i) {
+        p.iw_win[i] = (hi << 32) | ((unsigned long long)fe << 1);
+        p.iw_pend[i] = 1u;
+        p.iw_fcnt[i] = 0u;
+        p.iw_fcnt[k + i] = 0u;
+        p.iw_fmin[i] = INF32;
+        p.iw_fmin[k + i] = INF32;
+        p.ring[i & p.ring_mask] = (unsigned long long)(i * p.n + p.srcs[i]);
+    }
+    p.iw_misc[IW_ACTIVE] = k;
+    p.iw_misc[IW_MAXEP] = fe;
+    p.iw_misc[IW_ADVANCES] = k;
+    p.aq[AQ_HEAD] = 0u;
+    p.aq[AQ_TAIL] = k;
+    p.aq[AQ_DONE] = 0u;
+    p.aq[AQ_BUSY] = 0u;
+    p.aq[AQ_IDLE] = 0u;
+    sc.cnt[C_NEAR0] = 0u;
+    sc.cnt[C_NEAR1] = 0u;
+    r.in_count = 0u;
+    r.in_kind = 0u;
+    r.lo = 0ull;
+    r.hi = ~0ull;  // the shared test passes every key; each instance's window decides
+    r.async_bkt = 1u;
+    r.phase = PH_ASYNC;
+}
+
+// Position of this thread's entry in a pass of the independent-window drain:
+// warps 1..W-1 relax, warp 0 serves (its lanes take no entry).
+__device__ __forceinline__ u32 iw_item_slot() {
+    const u32 W = blockDim.x >> 5, warp = threadIdx.x >> 5;
+    return warp == 0u ? ~0u : (threadIdx.x & 31u) * (W - 1u) + (warp - 1u);
+}
+
+template <int AM>
+__device__ __forceinline__ void inst_drain(const RunParams& p, const Snap& s, Local& L, Coop& cs) {
+    __shared__ u32 s_src, s_h, s_n, s_spill, s_spill_from, s_spill_base, s_idle, s_j, s_nrel;
+    constexpr u32 CLM = CL_CAP - 1u;
+    const u32 G = gridDim.x, BS = blockDim.x, K = p.k;
+    const u32 RS = BS - 32u;  // entries per pass and thread row: the relaxing warps' lanes
+    u32* aq = p.aq;
+    Ctl* c = p.ctl;
+    const IwSh sh = iw_sh(&cs, K);
+    for (u32 i = threadIdx.x; i < K; i += BS) {
+        sh.lc[i] = 0u;
+        sh.fin[i] = 0u;
+        sh.held[i] = IW_FREE;
+    }
+    if (threadIdx.x == 0) {
+        *sh.adv_n = 0u;
+        *sh.rel_n = 0u;
+        s_idle = 0u;
+        s_nrel = 0u;
+    }
+    __syncthreads();
+    for (;;) {
+        if (threadIdx.x == 0) {
+            u32 tail = cs.cl_n;
+            if ((int)(tail - (cs.cl_head + CL_CAP)) > 0) tail = cs.cl_head + CL_CAP;
+            cs.cl_n = tail;
+            const u32 local = tail - cs.cl_head;
+            u32 src = 0, h = 0, n = 0, spill = 0;
+            if (local == 0u && *sh.adv_n == 0u && *sh.rel_n) {
+                // about to wait for work: release the marked holds now (they may be the
+                // last units of their windows)
+                __threadfence();
+                for (u32 q = 0; q < *sh.rel_n; ++q) iw_release(p, sh, sh.rel[q], K, c);
+                *sh.rel_n = 0u;
+            }
+            s_nrel = *sh.rel_n;  // the service warp releases these during the pass
+            *sh.rel_n = 0u;
+            if (*sh.adv_n) {
+                src = 4u;  // window advances first: they start the next bucket of an instance
+                n = 1u;
+                *sh.adv_n -= 1u;
+                s_j = sh.adv[*sh.adv_n];
+            } else if (local > 0u) {
+                src = 1u;
+                h = cs.cl_head;
+                const u32 cap = p.short_rows ? 2u * RS : RS;
+                n = local < cap ? local : cap;
+                const u32 backlog = local - n;
+                const u32 keep = p.spill_keep ? p.spill_keep : BS / 2u;
+                if (backlog >= 32u && (s_idle > 0u || backlog > keep))
+                    spill = s_idle > 0u ? backlog / 2u : backlog - keep;
+                cs.cl_head = h + n;
+            } else {
+                bool idle = false;
+                u64 t0 = global_timer_ns();
+                u32 beat = ld_relaxed(aq + AQ_BEAT);
+                u32 nap = 32u;
+                for (u32 spin = 1;; ++spin) {
+                    if ((spin & 15u) == 0u) {
+                        if (vload(&c->rd.status) != DS_OK) break;
+                        const u64 now = global_timer_ns();
+                        const u32 b = ld_relaxed(aq + AQ_BEAT);
+                        if (b != beat) {
+                            beat = b;
+                            t0 = now;
+                        } else if (now - t0 > p.timeout_ns) {
+                            flag_timeout(c, WS_DRAIN_IDLE);
+                            break;
+                        }
+                    }
+                    const u32 act = ld_acquire(p.iw_misc + IW_ACTIVE);
+                    const u32 t = ld_acquire(aq + AQ_TAIL);
+                    const u32 hh = ld_relaxed(aq + AQ_HEAD);
+                    if ((int)(t - hh) > 0) {
+                        nap = 32u;
+                        const u32 avail = t - hh;
+                        u32 want = (avail + G - 1u) / G;
+                        want = want < 32u ? 32u : want;
+                        want = want > RS ? RS : want;
+                        want = want > avail ? avail : want;
+                        if (atomicCAS(aq + AQ_HEAD, hh, hh + want) == hh) {
+                            src = 2u;
+                            h = hh;
+                            n = want;
+                            break;
+                        }
+                        continue;
+                    }
+                    if (act == 0u) break;  // every instance is finished
+                    if (!idle) {
+                        atomicAdd(aq + AQ_IDLE, 1u);
+                        idle = true;
+                    }
+                    __nanosleep(nap);
+                    nap = min(2u * nap, p.idle_ns ? p.idle_ns : 64u);
+                }
+                if (idle) atomicSub(aq + AQ_IDLE, 1u);
+            }
+            s_src = src;
+            s_h = h;
+            s_n = n;
+            s_spill = spill;
+            if (spill) {
+                s_spill_from = tail - spill;
+                s_spill_base = atomicAdd(aq + AQ_TAIL, spill);
+            }
+        }
+        __syncthreads();
+        const u32 src = s_src, h = s_h, n = s_n, spill = s_spill;
+        if (n == 0u) break;  // block-uniform (no hold is marked: the wait above released them)
+        if (threadIdx.x == 0) atomicAdd(aq + AQ_BEAT, 1u);
+        if (src == 4u) {
+            if (threadIdx.x < 32u) {  // the marked holds, before the advance's barriers
+                if (s_nrel) __threadfence();
+                for (u32 q = threadIdx.x; q < s_nrel; q += 32u) iw_release(p, sh, sh.rel[q], K, c);
+            }
+            iw_advance(p, s, s_j);
+            continue;
+        }
+        if (spill) {
+            // the newest part of the backlog goes to the ring: each entry gets a pending
+            // unit of its own before any of them is written, and leaves the CTA's count
+            const u32 from = s_spill_from, base = s_spill_base;
+            for (u32 b0 = 0; b0 < spill; b0 += BS) {
+                const u32 i = b0 + threadIdx.x;
+                const bool v = i < spill;
+                const u32 inst = v ? cs.cl[(from + i) & CLM] / p.n : 0u;
+                warp_add_keyed(p.iw_pend, inst, 1, v);
+                warp_add_keyed(sh.lc, inst, -1, v);
+            }
+            __threadfence();
+            __syncthreads();
+            for (u32 i = threadIdx.x; i < spill; i += BS) {
+                unsigned long long* slot = p.ring + ((base + i) & p.ring_mask);
+                const unsigned long long ent = ((unsigned long long)cs.cl_d[(from + i) & CLM] << 32) |
+                                               cs.cl[(from + i) & CLM];
+                if (atomicCAS(slot, RING_FREE, ent) != RING_FREE) {
+                    const u64 t0 = global_timer_ns();
+                    while (atomicCAS(slot, RING_FREE, ent) != RING_FREE) {
+                        if (global_timer_ns() - t0 > p.timeout_ns) {
+                            flag_timeout(c, WS_SPILL_SLOT);
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) cs.cl_n = from;
+            __syncthreads();
+        }
+        u32 u = 0, ib = 0, du = INF32, eb = 0, ee = 0, inst = 0;
+        unsigned long long w = 0ull, sw = 0ull;
+        bool act = false;
+        const u32 my = iw_item_slot();
+        unsigned long long ent = RING_FREE;
+        if (my < n) {
+            if (src == 1u) {
+                ent = ((unsigned long long)cs.cl_d[(h + my) & CLM] << 32) | cs.cl[(h + my) & CLM];
+            } else {
+                unsigned long long* slot = p.ring + ((h + my) & p.ring_mask);
+                ent = ld_relaxed64(slot);
+                if (ent == RING_FREE) {
+                    const u64 t0 = global_timer_ns();
+                    while ((ent = ld_relaxed64(slot)) == RING_FREE) {
+                        if (global_timer_ns() - t0 > p.timeout_ns) {
+                            flag_timeout(c, WS_RING_SLOT);
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                if (ent != RING_FREE) *slot = RING_FREE;
+            }
+        }
+        const u32 lw = (u32)ent;
+        const u32 gi = lw & ~IW_FAR_BIT;
+        const bool have = ent != RING_FREE && gi < p.total;
+        if (ent != RING_FREE && !have) atomicCAS(&c->rd.status, (u32)DS_OK, (u32)DS_NOT_CONVERGED);  // (cannot happen)
+        if (have) {
+            inst = gi / p.n;
+            sw = ld_state(p.state + gi);  // (issued together with the window word)
+            if (p.row_stride) asm volatile("prefetch.global.L1 [%0];" ::"l"(p.adj + ROW_ALIGN * (gi - inst * p.n)));
+            // claimed-list entries: the CTA holds the instance, its window is in shared memory
+            w = src == 1u ? sh.win[inst] : ld_relaxed64(p.iw_win + inst);
+        }
+        iw_take_ring(p, sh, inst, w, have && src == 2u);
+        warp_add_keyed(sh.fin, inst, 1, have);
+        if (have) act = take_iw(p, gi, inst, (lw & IW_FAR_BIT) != 0u, (u32)(ent >> 32), w, sw, L, u, ib, du, eb, ee);
+        // the second entry of this thread (claimed-list passes of more than a row of entries)
+        u32 u2 = 0, ib2 = 0, du2 = INF32, eb2 = 0, ee2 = 0, inst2 = 0;
+        unsigned long long w2 = 0ull;
+        bool act2 = false;
+        const bool have2 = src == 1u && my < RS && my + RS < n;
+        if (have2) {
+            const u32 q = (h + my + RS) & CLM;
+            const u32 gi2 = cs.cl[q];
+            inst2 = gi2 / p.n;
+            w2 = sh.win[inst2];
+            act2 = take_iw(p, gi2, inst2, false, cs.cl_d[q], w2, ld_state(p.state + gi2), L, u2, ib2, du2, eb2,
+                           ee2);
+        }
+        warp_add_keyed(sh.fin, inst2, 1, have2);
+        if (threadIdx.x < 32u) {
+            // service warp: the holds marked at the end of the last pass
+            if (threadIdx.x == 0) s_idle = ld_relaxed(aq + AQ_IDLE);
+            const u32 nr = s_nrel;
+            if (nr) __threadfence();  // the earlier passes' far pushes and state updates first
+            for (u32 q = threadIdx.x; q < nr; q += 32u) iw_release(p, sh, sh.rel[q], K, c);
+        }
+        relax_items<false, AM, 2>(p, s, act, u, du, ib, w, inst, eb, ee, L, cs, &cs, K_LIGHT);
+        if (n > RS)  // block-uniform
+            relax_items<false, AM, 2>(p, s, act2, u2, du2, ib2, w2, inst2, eb2, ee2, L, cs, &cs, K_LIGHT);
+        __syncthreads();  // every push of the pass has been performed
+        if (threadIdx.x < 32u) {
+            // entries finished; a hold the CTA no longer needs is marked for release
+            for (u32 j = threadIdx.x; j < K; j += 32u) {
+                const u32 f = sh.fin[j];
+                const u32 l = sh.lc[j] - f;
+                if (f) {
+                    sh.fin[j] = 0u;
+                    sh.lc[j] = l;
+                }
+                if (l == 0u && sh.held[j] == IW_HELD) {
+                    sh.held[j] = IW_RELEASING;
+                    sh.rel[atomicAdd(sh.rel_n, 1u)] = j;  // (each held instance at most once)
+                }
+            }
+            __syncwarp();
         }
     }
     if (threadIdx.x == 0) {
@@ -1853,6 +2380,13 @@ static __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, floa
         sc.bucket_rounds += 1u;
         r.near_epoch = old_near_epoch + 1u;  // every round pushes with a fresh stamp
         bool advance = false;
+        if (p.iw && ph == PH_ASYNC) {
+            // independent windows: the far stamps used so far (also after a failed
+            // run, so later runs never reuse them) and the window advances
+            const u32 ep = ld_relaxed(p.iw_misc + IW_MAXEP);
+            if (ep > r.far_epoch) r.far_epoch = ep;
+            sc.buckets = ld_relaxed(p.iw_misc + IW_ADVANCES);
+        }
         if (r.status != DS_OK) {
             r.phase = PH_DONE;
         } else if (rounds > sc.round_cap) {
@@ -1900,7 +2434,10 @@ static __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, floa
                 sc.bucket_rounds = 0u;
                 r.phase = PH_LIGHT;
                 r.async_bkt = 0u;
-                if (p.ring && !(p.mode == MODE_DELTA && p.policy)) enter_async(p, sc, r, 1u);
+                if (p.iw)
+                    enter_iw(p, sc, r);
+                else if (p.ring && !(p.mode == MODE_DELTA && p.policy))
+                    enter_async(p, sc, r, 1u);
                 if (p.mode == MODE_DELTA && (p.policy || p.trace)) {
                     // The first bucket is a decision point too: features of the
                     // seed window (nothing relaxed yet) and the graph.
@@ -1933,7 +2470,9 @@ static __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, floa
         } else if (ph == PH_ASYNC) {
             // the ring is drained: light arcs of the window are done
             sc.iterations += 1u;
-            if (r.heavy && sc.cnt[C_R]) {
+            if (p.iw) {
+                r.phase = PH_DONE;  // (independent windows: every instance is finished)
+            } else if (r.heavy && sc.cnt[C_R]) {
                 r.in_count = sc.cnt[C_R];
                 r.phase = PH_HEAVY;
             } else {
@@ -2203,6 +2742,8 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
     __shared__ float s_feat[POL_IN];
     __shared__ float act0[POL_H], act1[POL_H];
     Local L;
+    // independent bucket windows exist for SSSP with the hybrid mapping's CTA passes
+    constexpr bool IW_KERNEL = !ASTAR && MAP == 2 && !WD;
     // Failure test: with CTA 0 absent no barrier completes; every other CTA's
     // wait runs into its time limit and the run ends with DS_TIMEOUT.
     if (p.test_absent_cta && blockIdx.x == 0) return;
@@ -2245,6 +2786,8 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
             round_naive<ASTAR, AM>(p, s, L);
         } else if (ph == PH_COMPACT) {
             round_compact(p, s, cs);
+        } else if (ph == PH_ASYNC && IW_KERNEL && p.iw) {
+            if constexpr (IW_KERNEL) inst_drain<AM>(p, s, L, cs);
         } else if (ph == PH_ASYNC) {
             if constexpr (WD) wq_reset(cs);
             if (s.in_count) {

@@ -314,6 +314,9 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
     s->ring_mask = (u32)(ring - 1);
     TRY(s->dalloc(&s->d_aq, (u64)AQ_WORDS));
     TRYC(cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, s->stream));
+    // Independent bucket windows: per-instance windows, pending counts and far-pile
+    // counters (every run that uses them rewrites the block first).
+    if (K <= IW_MAX_INST && Kn < (u64)IW_FAR_BIT) TRY(s->dalloc(&s->d_iw, iw_words(K)));
     // Hub records: every instance's hub rows once per round, twice over for
     // re-published rows of an asynchronous drain (overflow falls back to the CTA).
     if (s->hub_rows) {
@@ -390,11 +393,11 @@ void sanitize_options(pfg_options& o) {
     if (o.block_size < 32 || o.block_size > 1024 || (o.block_size % 32) != 0) o.block_size = 256;
     if (o.mapping < 0 || o.mapping > 2) o.mapping = PFG_MAP_HYBRID;
     if (o.atomic < 0 || o.atomic > 2) o.atomic = PFG_ATOMIC_MIN_RBA;
-    if (o.schedule < 0 || o.schedule > 3) o.schedule = PFG_SCHEDULE_AUTO;
+    if (o.schedule < 0 || o.schedule > 4) o.schedule = PFG_SCHEDULE_AUTO;
 }
 
-int blocks_per_sm_for(const pfg_options& o, bool astar, int map) {
-    int bps = persistent_blocks_per_sm(astar, o.atomic, map, o.block_size);
+int blocks_per_sm_for(const pfg_options& o, bool astar, int map, bool iw, u32 k) {
+    int bps = persistent_blocks_per_sm(astar, o.atomic, map, o.block_size, false, iw ? k : 0u);
     if (bps <= 0) return 0;
     // Default: fill each SM up to 1024 resident threads (more CTAs only make
     // the grid barrier slower on this latency-bound kernel).
@@ -441,9 +444,10 @@ bool async_buckets_for(const pfg_options& o, int mode) {
 
 }  // namespace pfg
 
-// Resets the stamp words when the epoch counters approach 2^32.
-static pfg_status maybe_reset_epochs(pfg_solver* s) {
-    if (s->epoch_hint < 0xF0000000u) return PFG_OK;
+// Resets the stamp words when the epoch counters approach 2^32 (2^31 for a run
+// under independent windows, whose far epochs share a word with a pile index).
+static pfg_status maybe_reset_epochs(pfg_solver* s, bool iw) {
+    if (s->epoch_hint < (iw ? 0x70000000u : 0xF0000000u)) return PFG_OK;
     const u64 Kn = (u64)s->K * s->n;
     for (int i = 0; i < 3; ++i) PFG_CUDA(cudaMemsetAsync(s->d_stamp[i], 0, Kn * 4, s->stream));
     Ctl tmp;
@@ -478,12 +482,32 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     if (o.policy == PFG_POLICY_LEARNED && !s->has_net)
         return fail(PFG_ERR_INVALID_ARGUMENT, "learned policy requested but no network is loaded");
     PFG_CUDA(cudaSetDevice(s->device));
-    pfg_status st = maybe_reset_epochs(s);
-    if (st != PFG_OK) return st;
 
     const int mode = o.algo == PFG_ALGO_NAIVE ? MODE_NAIVE
                    : o.algo == PFG_ALGO_FRONTIER ? MODE_FRONTIER : MODE_DELTA;
-    const u32 delta = mode == MODE_DELTA ? (o.delta ? o.delta : auto_delta_of(s->avg_w, s->avg_deg)) : 0u;
+    u32 delta = mode == MODE_DELTA ? (o.delta ? o.delta : auto_delta_of(s->avg_w, s->avg_deg)) : 0u;
+    // Independent bucket windows: multi-source Delta-stepping with the hybrid mapping's
+    // CTA passes, every arc light (Delta >= the largest weight), no hub rows and no
+    // learned policy or trace. Each instance's run is then bound by its own buckets, one
+    // after the other, so the automatic Delta is widened (4x, PFG_IW_DELTA_MULT): the
+    // extra relaxations of wider windows overlap with other instances' work (1000 x 1000
+    // grid, 256 sources: 56.9 ms with a shared window at the automatic Delta, 35.9 ms).
+    // The automatic schedule takes them from 128 instances on (PFG_INST_WINDOWS: the
+    // smallest batch, 0 = never), where they measured faster; PFG_SCHEDULE_INSTANCE asks
+    // for them at any batch size and falls back to a shared window where they do not apply.
+    const u64 iw_delta = o.delta ? (u64)o.delta
+                                 : (u64)delta * (u64)std::max(1, env_int("PFG_IW_DELTA_MULT", 4));
+    const bool iw_fits = mode == MODE_DELTA && !astar && k > 1 && s->d_iw && k <= IW_MAX_INST &&
+                         (u64)k * s->n < (u64)IW_FAR_BIT && iw_delta >= s->maxw && iw_delta < 0x80000000ull &&
+                         o.mapping == PFG_MAP_HYBRID && o.policy != PFG_POLICY_LEARNED && !d_trace &&
+                         s->max_deg <= 8u * (u32)o.block_size &&
+                         o.block_size >= 64;  // (warp 0 of a CTA serves, the others relax)
+    const int iw_min = env_int("PFG_INST_WINDOWS", 128);
+    const bool iw = iw_fits && (o.schedule == PFG_SCHEDULE_INSTANCE ||
+                                (o.schedule == PFG_SCHEDULE_AUTO && iw_min > 0 && (int)k >= iw_min));
+    if (iw) delta = (u32)iw_delta;
+    pfg_status st = maybe_reset_epochs(s, iw);
+    if (st != PFG_OK) return st;
 
     // Control block for this run (the persistent epoch part is left alone).
     Ctl* c = s->h_ctl;
@@ -580,12 +604,21 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
         p.aq = s->d_aq;
     }
     configure_drain(p, o.schedule, s->d_hubs, s->hub_cap, s->max_deg, s->d_aq, map, block);
+    if (iw) {
+        p.iw = 1u;
+        p.iw_win = reinterpret_cast<unsigned long long*>(s->d_iw);
+        p.iw_pend = s->d_iw + 2u * k;
+        p.iw_fcnt = s->d_iw + 3u * k;
+        p.iw_fmin = s->d_iw + 5u * k;
+        p.iw_misc = s->d_iw + 7u * k;
+        p.hubs = nullptr;  // (no row reaches the grid tier: max_deg <= 8 blocks)
+    }
     // A single source on a graph of short rows is bound by the latency of its hops: its
     // entries are relaxed without the state read (1000 x 1000 grid: 6.22 -> 5.79 ms); with
     // more instances the stale entries' extra work costs more than it saves (K = 64:
     // 14.6 -> 18.3 ms), so they keep the check.
     p.trust_entries = (k == 1 && p.short_rows && env_int("PFG_TRUST_ENTRIES", 1) != 0) ? 1u : 0u;
-    const int bps = blocks_per_sm_for(o, astar != 0, map);
+    const int bps = blocks_per_sm_for(o, astar != 0, map, iw, k);
     if (bps <= 0) return fail(PFG_ERR_CUDA, "occupancy query failed for block size %d", block);
     const int grid = s->sm_count * bps;
     // Eager propagation pays in rounds that leave most of the GPU idle: inputs
@@ -634,6 +667,11 @@ static pfg_status complete_run(pfg_solver* s, pfg_stats* stats_out) {
         stats_out->rounds = c->rounds;
     }
     const u32 status = c->rd.status;
+    if (status != DS_OK && status != DS_TIMEOUT) {
+        // (a run that ended early may leave ring entries behind)
+        cudaMemsetAsync(s->d_ring, 0xFF, ((u64)s->ring_mask + 1) * 8, s->stream);
+        cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, s->stream);
+    }
     if (status == DS_TIMEOUT) {
         // A wait gave up: reset the naive masks and the ring so the next run starts clean.
         const u64 words = (u64)s->n / 32 + 1;

@@ -67,7 +67,7 @@ def test_grid100_all_sources(oracle, grid100, grid100_solver, algo):
         check_sssp(oracle, grid100, src, res)
 
 
-SCHEDULES = [Schedule.Rounds, Schedule.Async, Schedule.Warp]
+SCHEDULES = [Schedule.Rounds, Schedule.Async, Schedule.Warp, Schedule.Instance]
 
 
 @pytest.mark.parametrize("mapping,atomic", list(itertools.product(list(Mapping), list(AtomicMode))))
@@ -101,12 +101,66 @@ def test_grid300_async_batch(oracle, block):
     refs = [oracle.sssp_canonical(g, src) for src in srcs]
     with pf.GpuSolver(g, 8) as s:
         for atomic in (AtomicMode.MinRBA, AtomicMode.MinNoCheck):
-            for sched in (Schedule.Async, Schedule.Warp):
+            for sched in (Schedule.Async, Schedule.Warp, Schedule.Instance):
                 _, _, state = s.run_state(srcs, GpuOptions(blockSize=block, atomic=atomic, schedule=sched))
                 dist, parent = pf.unpack(state)
                 for i, (d_ref, p_can) in enumerate(refs):
                     assert np.array_equal(dist[i * g.n:(i + 1) * g.n], d_ref), (block, atomic, sched, i)
                     assert np.array_equal(parent[i * g.n:(i + 1) * g.n], p_can), (block, atomic, sched, i)
+
+
+def _check_batch(oracle, g, srcs, state):
+    dist, parent = pf.unpack(state)
+    for i, src in enumerate(srcs):
+        d_ref, p_can = oracle.sssp_canonical(g, src)
+        assert np.array_equal(dist[i * g.n:(i + 1) * g.n], d_ref), i
+        assert np.array_equal(parent[i * g.n:(i + 1) * g.n], p_can), i
+
+
+@pytest.mark.parametrize("k", [2, 3, 17, 64, 130])
+def test_instance_windows_grid(oracle, k):
+    # a bucket window per instance: every instance's own far piles, window advances and
+    # hand-over of pending units (k >= 64: CTAs hold entries of many instances at once;
+    # k = 130: the automatic schedule's own choice); duplicate sources and a Delta equal
+    # to the largest weight (the smallest that applies)
+    g = pf.grid(120, 90, SEED + 11)
+    srcs = pf.uniform_vertices(g.n, k, SEED + k).tolist()
+    srcs[-1] = srcs[0]
+    maxw = int(g.maxW)
+    with pf.GpuSolver(g, k) as s:
+        for delta in (0, maxw, 4 * maxw):
+            for block in (64, 256):
+                stats, _, state = s.run_state(srcs, GpuOptions(delta=delta, blockSize=block,
+                                                               schedule=Schedule.Instance))
+                _check_batch(oracle, g, srcs, state)
+                assert stats.buckets >= k  # every instance's first window counts
+        # the automatic schedule (independent windows from 128 sources) and a shared window
+        for sched in (Schedule.Auto, Schedule.Async):
+            _, _, state = s.run_state(srcs, GpuOptions(schedule=sched))
+            _check_batch(oracle, g, srcs, state)
+
+
+def test_instance_windows_fallbacks_and_long_rows(oracle, rmat12, rmat12_solver):
+    # R-MAT rows above 32 arcs go through the CTA-cooperative dealing (the window word
+    # travels in shared memory); Delta below the largest weight and the learned-policy
+    # exclusions fall back to one shared window; results are identical either way
+    srcs = [int(v) for v in pf.pick_sources(rmat12, 8, SEED + 5)]
+    maxw = int(rmat12.maxW)
+    for delta in (maxw, 3 * maxw, 16):
+        for atomic in (AtomicMode.MinRBA, AtomicMode.CasRBA, AtomicMode.MinNoCheck):
+            _, _, state = rmat12_solver.run_state(srcs, GpuOptions(delta=delta, atomic=atomic,
+                                                                   schedule=Schedule.Instance))
+            _check_batch(oracle, rmat12, srcs, state)
+
+
+def test_instance_windows_repeated_runs(oracle, grid100, grid100_solver):
+    # far stamps continue across runs of every schedule: alternate them on one solver
+    srcs = sources_c0(grid100)
+    for rep in range(3):
+        for sched in (Schedule.Instance, Schedule.Async, Schedule.Rounds, Schedule.Instance):
+            _, _, state = grid100_solver.run_state(srcs, GpuOptions(schedule=sched))
+            _check_batch(oracle, grid100, srcs, state)
+        check_sssp(oracle, grid100, 77, grid100_solver.sssp(77, GpuOptions(schedule=Schedule.Instance)))
 
 
 @pytest.mark.parametrize("eager", [0, 1, 3, 16, 64])
