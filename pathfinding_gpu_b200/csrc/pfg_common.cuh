@@ -145,7 +145,9 @@ struct __align__(16) Ctl {
     u32 cnt[C_COUNT];  // queue tails
     unsigned long long stats[4];  // edges, atomics, updates, pushes
     u64 bucket_edges;  // edges scanned up to the start of the bucket (policy feature)
-    u64 bucket_edges_acc;  // edges scanned so far, flushed every round when the policy runs
+    // edges scanned so far, flushed every round when the policy runs: one atomicAdd per CTA
+    // into stripe (CTA index mod 16), so no single word takes thousands of atomics a round
+    u64 edge_stripe[16];
     // --- persistent across runs ---
     u32 persist;       // marker: everything from here on survives between runs
     u32 near_epoch;    // last stamp used by near pushes

@@ -2221,11 +2221,13 @@ template <int NI, int NO, bool RELU>
 __device__ __forceinline__ void policy_layer(const float* __restrict__ w, const float* __restrict__ b,
                                              const float* in, float* out) {
     const u32 t = threadIdx.x, BS = blockDim.x;
-    const u32 G = BS >= 256u ? 4u : 1u;
+    constexpr u32 G = 4u;  // (a compile-time stride: a thread's weight loads are all in flight at once)
     const u32 part = t & (G - 1u);
     for (u32 j = t / G; j < (u32)NO; j += BS / G) {  // uniform within each warp (NO * G % 32 == 0)
         float a = 0.f;
-        for (u32 i = part; i < (u32)NI; i += G) a = fmaf(__ldg(w + j * NI + i), in[i], a);
+#pragma unroll
+        for (u32 i = 0; i < (u32)NI; i += G)
+            if (i + part < (u32)NI) a = fmaf(__ldg(w + j * NI + i + part), in[i + part], a);
         for (u32 o = G >> 1; o > 0; o >>= 1) a += __shfl_down_sync(FULL, a, o, G);
         if (part == 0) {
             a += __ldg(b + j);
@@ -2276,7 +2278,8 @@ static __device__ u32 policy_pick(const PolicyNet* net, const float* feat, float
 static __device__ void decision_features(const RunParams& p, Ctl& sc, const Rd& r, u32 fn, u64 est, float* f,
                                          u32* s_flag, u32 far_pile) {
     const double aw = p.avg_w > 0.0 ? p.avg_w : 1.0;
-    const u64 edges_now = sc.bucket_edges_acc;
+    u64 edges_now = 0;
+    for (int i = 0; i < 16; ++i) edges_now += sc.edge_stripe[i];
     const double arcs = (double)(edges_now - sc.bucket_edges);
     f[0] = log2f(1.f + (float)fn);
     f[1] = log2f(1.f + (float)sc.bucket_near);
@@ -2365,6 +2368,13 @@ static __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, floa
                            float* act1) {
     const u32 t = threadIdx.x;
     __shared__ u64 s_key0;
+    if (p.policy && p.net) {
+        // the network's 40 KB into this CTA's L1 while the decision's features are
+        // gathered (its layers then read them without an L2 round trip each)
+        const char* w = reinterpret_cast<const char*>(p.net);
+        for (u32 off = t * 128u; off < (u32)sizeof(PolicyNet); off += blockDim.x * 128u)
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(w + off));
+    }
     // s_flag[0]: 0 = no bucket advance, 1 = advance with the policy, 2 = fixed Delta
     if (t == 0) {
         Rd& r = sc.rd;
@@ -2652,19 +2662,23 @@ __device__ __forceinline__ void grid_barrier(const RunParams& p, Snap& s, Local&
                              float* s_feat, float* act0, float* act1) {
     __syncthreads();
     Ctl* c = p.ctl;
-    const u64 fmin = block_min_u64(L.fmin, red);
-    L.fmin = ~0ull;
-    __shared__ u32 s_last, s_gen;
-    if (p.policy || p.trace) {
-        // Arcs scanned this round (for the policy's per-bucket work feature):
-        // each thread's count since the last flush, one atomicAdd per warp.
+    __shared__ u32 s_last, s_gen, s_edges;
+    const bool count_edges = p.policy || p.trace;
+    if (count_edges) {
+        // Arcs scanned this round (for the policy's per-bucket work feature): each
+        // thread's count since the last flush, summed per warp, then per CTA.
+        if (threadIdx.x == 0) s_edges = 0u;
+        __syncthreads();
         u32 x = L.edges - L.edges_flushed;
         L.edges_flushed = L.edges;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(FULL, x, o);
-        if ((threadIdx.x & 31u) == 0 && x)
-            atomicAdd((unsigned long long*)&c->bucket_edges_acc, (unsigned long long)x);
+        if ((threadIdx.x & 31u) == 0 && x) atomicAdd(&s_edges, x);
     }
+    const u64 fmin = block_min_u64(L.fmin, red);  // (its barrier also completes the sums above)
+    L.fmin = ~0ull;
+    if (count_edges && threadIdx.x == 0 && s_edges)
+        atomicAdd((unsigned long long*)&c->edge_stripe[blockIdx.x & 15u], (unsigned long long)s_edges);
     if (threadIdx.x == 0) {
         if (fmin != ~0ull) atomicMin((unsigned long long*)&c->far_min[s.far_out], (unsigned long long)fmin);
         __threadfence();
