@@ -28,7 +28,8 @@ HEADERS = ["pfg_common.cuh", "pfg_kernels.h", "pfg_internal.h", "pfg_persistent.
 # The persistent kernel's instantiations, one object per (A*, atomic mode, part):
 # compiled from one source in parallel (each instantiation is a large fully inlined kernel).
 PERSISTENT = "pfg_persistent.cu"
-VARIANTS = [(a, am, part) for a in (0, 1) for am in (0, 1, 2) for part in (0, 1, 2)]
+VARIANTS = [(a, am, part) for a in (0, 1) for am in (0, 1, 2) for part in (0, 1, 2)] + \
+           [(0, am, 3) for am in (0, 1, 2)]  # part 3: independent bucket windows (SSSP only)
 
 
 def _nvcc() -> str:

@@ -11,7 +11,8 @@
 namespace pfg {
 // Defined in pfg_persistent.cu, one object per (A*, atomic mode, part):
 // part 0 = Thread and Warp mappings (map 0 / 1), part 1 = Hybrid mapping,
-// part 2 = Hybrid mapping with warp-worker drains.
+// part 2 = Hybrid mapping with warp-worker drains, part 3 = Hybrid mapping with
+// independent bucket windows (SSSP only).
 #define PFG_DECLARE_GETTERS(A, AM)                        \
     const void* persistent_kernel_##A##_##AM##_0(int map); \
     const void* persistent_kernel_##A##_##AM##_1(int map); \
@@ -23,6 +24,9 @@ PFG_DECLARE_GETTERS(1, 0)
 PFG_DECLARE_GETTERS(1, 1)
 PFG_DECLARE_GETTERS(1, 2)
 #undef PFG_DECLARE_GETTERS
+const void* persistent_kernel_0_0_3(int map);
+const void* persistent_kernel_0_1_3(int map);
+const void* persistent_kernel_0_2_3(int map);
 }  // namespace pfg
 
 // ===========================================================================
@@ -32,10 +36,15 @@ namespace pfg {
 
 typedef const void* (*KernelGetter)(int);
 
-// wd: the warp-drain instantiation (hybrid mapping only).
-static const void* kernel_for(bool astar, int am, int map, bool wd = false) {
+// wd: the warp-drain instantiation, iw: the independent-window one (hybrid mapping only).
+static const void* kernel_for(bool astar, int am, int map, bool wd = false, bool iw = false) {
     if (am < 0 || am > 2) am = 0;
     if (map < 0 || map > 2) map = 2;
+    if (iw && !astar && map == 2) {
+        static const KernelGetter iw_table[3] = {persistent_kernel_0_0_3, persistent_kernel_0_1_3,
+                                                 persistent_kernel_0_2_3};
+        return iw_table[am](map);
+    }
     static const KernelGetter table[2][3][3] = {
         {{persistent_kernel_0_0_0, persistent_kernel_0_0_1, persistent_kernel_0_0_2},
          {persistent_kernel_0_1_0, persistent_kernel_0_1_1, persistent_kernel_0_1_2},
@@ -50,16 +59,17 @@ static const void* kernel_for(bool astar, int am, int map, bool wd = false) {
 // Dynamic shared memory of the persistent kernel (one Coop per CTA); the
 // opt-in above 48 KB is set once per instantiation and device (not a stream
 // operation, so launches inside a stream capture need nothing more).
-static cudaError_t allow_coop_smem(bool astar, int am, int map, bool wd) {
-    static std::atomic<unsigned> done[64];  // bit (wd, astar, am, map) per device
+static cudaError_t allow_coop_smem(bool astar, int am, int map, bool wd, bool iw = false) {
+    static std::atomic<unsigned> done[64];  // bit (iw | wd, astar, am, map) per device
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     const bool w = wd && map == 2;
-    const unsigned bit = 1u << ((w ? 18 : 0) + (astar ? 9 : 0) + 3 * am + map);
+    const bool v = iw && !astar && map == 2;
+    const unsigned bit = 1u << (v ? 27 + am : (w ? 18 : 0) + (astar ? 9 : 0) + 3 * am + map);
     if (dev < 64 && (done[dev].load() & bit)) return cudaSuccess;
     // (room for the independent-window arrays of the largest batch that uses them)
-    e = cudaFuncSetAttribute(kernel_for(astar, am, map, w), cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(kernel_for(astar, am, map, w, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(iw_smem_offset(MAX_BS) + iw_smem_bytes(IW_MAX_INST)));
     if (e == cudaSuccess && dev < 64) done[dev].fetch_or(bit);
     return e;
@@ -76,9 +86,9 @@ cudaError_t launch_persistent(const RunParams& p, bool astar, int am, int map, i
     if (map < 0 || map > 2) map = 2;
     // the warp drain exists for the hybrid mapping only, and its pushes need its kernel
     if (p.warp_drain && map != 2) return cudaErrorInvalidValue;
-    const bool wd = p.warp_drain != 0u;
-    const void* k = kernel_for(astar, am, map, wd);
-    const cudaError_t ea = allow_coop_smem(astar, am, map, wd);
+    const bool wd = p.warp_drain != 0u, iw = p.iw != 0u;
+    const void* k = kernel_for(astar, am, map, wd, iw);
+    const cudaError_t ea = allow_coop_smem(astar, am, map, wd, iw);
     if (ea != cudaSuccess) return ea;
     if (p.iw && (astar || map != 2 || wd || p.k > IW_MAX_INST)) return cudaErrorInvalidValue;
     cfg.dynamicSmemBytes = p.iw ? iw_smem_offset((u32)block) + iw_smem_bytes(p.k) : coop_bytes((u32)block);
@@ -97,9 +107,9 @@ int persistent_blocks_per_sm(bool astar, int am, int map, int block, bool wd, u3
     int nb = 0;
     if (am < 0 || am > 2) am = 0;
     if (map < 0 || map > 2) map = 2;
-    const void* k = kernel_for(astar, am, map, wd);
+    const void* k = kernel_for(astar, am, map, wd, iw_k > 0u);
     const size_t dyn = iw_k ? iw_smem_offset((u32)block) + iw_smem_bytes(iw_k) : coop_bytes((u32)block);
-    if (allow_coop_smem(astar, am, map, wd) != cudaSuccess ||
+    if (allow_coop_smem(astar, am, map, wd, iw_k > 0u) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block, dyn) != cudaSuccess) {
         cudaGetLastError();
         return 0;

@@ -311,10 +311,27 @@ __device__ __forceinline__ bool wq_push(Coop& cs, unsigned long long ent, const 
 // Appends gv, which this thread has just claimed (near: for the current
 // window; else: for the far pile), to the claimed list, the ring, or a queue;
 // nd is its new distance (carried by entries of asynchronous buckets).
+// IW: independent windows (near entries only; cl is the CTA's Coop): the entry is
+// counted as the CTA's, or gets a pending unit of its own when it overflows.
+template <bool IW = false>
 __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, u32 gv, u32 nd, bool near,
                                              u32 inst, Local& L, Coop* cl) {
     Ctl* c = p.ctl;
     L.pushes++;
+    if constexpr (IW) {
+        const u32 slot = atomicAdd(&cl->cl_n, 1u);
+        if (slot - cl->cl_head < CL_CAP) {
+            cl->cl[slot & (CL_CAP - 1u)] = gv;
+            cl->cl_d[slot & (CL_CAP - 1u)] = nd;
+            atomicAdd(iw_sh(cl, p.k).lc + inst, 1u);  // held by this CTA
+            return;
+        }
+        atomicAdd(p.iw_pend + inst, 1u);  // counted before the entry can be taken
+        __threadfence();
+        if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, ((unsigned long long)nd << 32) | gv, p.timeout_ns))
+            flag_timeout(c, WS_RING_PUSH);
+        return;
+    }
     if (!near) {
         queue_push(p.farq[s.far_out], &c->cnt[C_FAR0 + s.far_out], gv);
         if (p.inst_far_cnt) atomicAdd(p.inst_far_cnt + inst, 1u);
@@ -333,15 +350,10 @@ __device__ __forceinline__ void push_claimed(const RunParams& p, const Snap& s, 
         if (slot - cl->cl_head < CL_CAP) {
             cl->cl[slot & (CL_CAP - 1u)] = gv;
             cl->cl_d[slot & (CL_CAP - 1u)] = nd;
-            if (p.iw) atomicAdd(iw_sh(cl, p.k).lc + inst, 1u);  // held by this CTA
             return;
         }
     }
     if (s.async_bkt) {
-        if (p.iw) {  // a pending unit of its own, counted before the entry can be taken
-            atomicAdd(p.iw_pend + inst, 1u);
-            __threadfence();
-        }
         if (!ring_push(p.ring, p.ring_mask, p.aq + AQ_TAIL, ((unsigned long long)nd << 32) | gv, p.timeout_ns))
             flag_timeout(c, WS_RING_PUSH);
         return;
@@ -370,12 +382,19 @@ __device__ __forceinline__ void iw_far_push(const RunParams& p, u32 gi, u32 inst
 
 // After gv's distance was lowered to a value of key `key`: flag it (prefix-scan
 // compaction) or claim it for the window / the far pile and queue it. ub: the
-// A* pruning bound, or (SSSP) the window word of the item's instance under
-// independent windows (~0 otherwise).
-template <bool ASTAR>
+// A* pruning bound; under independent windows (IW) the window word of the
+// item's instance, whose high half is the window end.
+template <bool ASTAR, bool IW = false>
 __device__ __forceinline__ void after_improve(const RunParams& p, const Snap& s, u32 gv, u64 key, u32 nd,
                                               u32 inst, u64 ub, Local& L, Coop* cl) {
     L.updates++;
+    if constexpr (IW) {
+        if (key < (ub >> 32))
+            push_claimed<true>(p, s, gv, nd, true, inst, L, cl);
+        else
+            iw_far_push(p, gv, inst, (u32)key, ub, L);
+        return;
+    }
     if (p.mode == MODE_NAIVE) {  // Bellman-Ford sweep: the head is active in the next sweep
         atomicOr(p.naive_mask[s.naive_in ^ 1u] + (gv >> 5), 1u << (gv & 31u));
         if (vload(&p.ctl->changed) == 0u) p.ctl->changed = 1u;
@@ -386,16 +405,7 @@ __device__ __forceinline__ void after_improve(const RunParams& p, const Snap& s,
         L.pushes++;
         return;
     }
-    // (independent windows: the shared window is unbounded and the instance's
-    // window end is the high half of ub; SSSP runs otherwise pass ub = ~0)
-    const bool near = key < s.hi && (ASTAR || key < (ub >> 32));
-    if (!ASTAR && p.iw) {
-        if (near)
-            push_claimed(p, s, gv, nd, true, inst, L, cl);
-        else
-            iw_far_push(p, gv, inst, (u32)key, ub, L);
-        return;
-    }
+    const bool near = key < s.hi;
     if (!near) L.fmin = key < L.fmin ? key : L.fmin;
     if (near && s.async_bkt) {
         // Asynchronous bucket: no claim. Every strict improvement queues an
@@ -428,20 +438,20 @@ __device__ __forceinline__ bool arc_candidate(const RunParams& p, u32 du, u64 ub
     return true;
 }
 
-template <bool ASTAR, int AM>
+template <bool ASTAR, int AM, bool IW = false>
 __device__ __forceinline__ void relax_arc(const RunParams& p, const Snap& s, u32 u, u32 du,
                                           u32 ib, u64 ub, u32 inst, u32 v, u32 w, Local& L, Coop* cl) {
     u64 nd = 0, key = 0;
     if (!arc_candidate<ASTAR>(p, du, ub, inst, v, w, L, nd, key)) return;
     const u32 gv = ib + v;
     if (!relax_state<AM>(p.state + gv, (u32)nd, u, L.atomics)) return;
-    after_improve<ASTAR>(p, s, gv, key, (u32)nd, inst, ub, L, cl);
+    after_improve<ASTAR, IW>(p, s, gv, key, (u32)nd, inst, ub, L, cl);
 }
 
 // Two arcs of one lane relaxed together: both state updates are issued before
 // either result is used, so their L2 round trips overlap (same outcome as two
 // relax_arc calls in a row).
-template <bool ASTAR, int AM>
+template <bool ASTAR, int AM, bool IW = false>
 __device__ __forceinline__ void relax_arc_pair(const RunParams& p, const Snap& s, bool va, u32 ua, u32 dua,
                                                u32 iba, u64 uba, u32 insta, uint2 aa, bool vb, u32 ub2, u32 dub,
                                                u32 ibb, u64 ubb, u32 instb, uint2 ab, Local& L, Coop* cl) {
@@ -469,8 +479,8 @@ __device__ __forceinline__ void relax_arc_pair(const RunParams& p, const Snap& s
         ia = ta && st_dist(oa) > (u32)nda;
         ibt = tb && st_dist(ob) > (u32)ndb;
     }
-    if (ia) after_improve<ASTAR>(p, s, gva, keya, (u32)nda, insta, uba, L, cl);
-    if (ibt) after_improve<ASTAR>(p, s, gvb, keyb, (u32)ndb, instb, ubb, L, cl);
+    if (ia) after_improve<ASTAR, IW>(p, s, gva, keya, (u32)nda, insta, uba, L, cl);
+    if (ibt) after_improve<ASTAR, IW>(p, s, gvb, keyb, (u32)ndb, instb, ubb, L, cl);
 }
 
 // Thread tier: one thread walks its own arcs [eb, ee) with 128-bit loads
@@ -638,7 +648,7 @@ __device__ __forceinline__ bool take_item(const RunParams& p, const Snap& s, u32
 // numbered with a block-wide scan and dealt out one per thread, so every arc
 // of a road-graph vertex and every slice of a hub row is relaxed in parallel
 // (one dependent chain per arc). Called by every thread of the CTA.
-template <bool ASTAR, int AM>
+template <bool ASTAR, int AM, bool IW = false>
 __device__ __forceinline__ void relax_chunk_edges(const RunParams& p, const Snap& s, bool act, u32 u,
                                                   u32 du, u32 ib, u64 ub, u32 inst, u32 eb, u32 ee,
                                                   Local& L, Coop& cs, Coop* cl) {
@@ -674,7 +684,7 @@ __device__ __forceinline__ void relax_chunk_edges(const RunParams& p, const Snap
         }
         const u32 e = c_eb[lo] + (j - c_off[lo]);
         const uint2 a = __ldg(p.adj + e);
-        relax_arc<ASTAR, AM>(p, s, c_u[lo], c_du[lo], c_ib[lo], c_ub[lo], c_inst[lo], a.x, a.y, L, cl);
+        relax_arc<ASTAR, AM, IW>(p, s, c_u[lo], c_du[lo], c_ib[lo], c_ub[lo], c_inst[lo], a.x, a.y, L, cl);
     }
     __syncthreads();
 }
@@ -710,7 +720,7 @@ __device__ __forceinline__ u32 item_slot() {
 // by a 5-step shuffle search), with no block barrier. Used when no item of the
 // CTA has more than WARP_ROW_MAX selected arcs, so a warp never carries a hub.
 constexpr u32 WARP_ROW_MAX = 32;
-template <bool ASTAR, int AM>
+template <bool ASTAR, int AM, bool IW = false>
 __device__ __forceinline__ void relax_items_warp(const RunParams& p, const Snap& s, bool act, u32 u, u32 du,
                                                  u32 ib, u64 ub, u32 inst, u32 eb, u32 ee, Local& L, Coop* cl) {
     const u32 lane = threadIdx.x & 31u;
@@ -741,14 +751,15 @@ __device__ __forceinline__ void relax_items_warp(const RunParams& p, const Snap&
         const u32 bib = __shfl_sync(FULL, ib, lob), binst = __shfl_sync(FULL, inst, lob);
         const u32 beb = __shfl_sync(FULL, eb, lob) + (jb - __shfl_sync(FULL, off, lob));
         u64 aub = ~0ull, bub = ~0ull;
-        if (ASTAR || p.iw) {  // (warp-uniform)
+        if constexpr (ASTAR || IW) {
             aub = __shfl_sync(FULL, ub, loa);
             bub = __shfl_sync(FULL, ub, lob);
         }
         const bool vb = jb < total;
         const uint2 aa = __ldg(p.adj + aeb);
         const uint2 ab = vb ? __ldg(p.adj + beb) : make_uint2(0u, PAD_W);
-        relax_arc_pair<ASTAR, AM>(p, s, true, au, adu, aib, aub, ainst, aa, vb, bu, bdu, bib, bub, binst, ab, L, cl);
+        relax_arc_pair<ASTAR, AM, IW>(p, s, true, au, adu, aib, aub, ainst, aa, vb, bu, bdu, bib, bub, binst, ab, L,
+                                      cl);
         j0 += 64u;
     }
     for (; j0 < total; j0 += 32) {  // warp-uniform
@@ -764,17 +775,17 @@ __device__ __forceinline__ void relax_items_warp(const RunParams& p, const Snap&
         const u32 wib = __shfl_sync(FULL, ib, lo), winst = __shfl_sync(FULL, inst, lo);
         const u32 web = __shfl_sync(FULL, eb, lo), woff = __shfl_sync(FULL, off, lo);
         u64 wub = ~0ull;
-        if (ASTAR || p.iw) wub = __shfl_sync(FULL, ub, lo);
+        if constexpr (ASTAR || IW) wub = __shfl_sync(FULL, ub, lo);
         if (j < total) {
             const uint2 a = __ldg(p.adj + web + (j - woff));
-            relax_arc<ASTAR, AM>(p, s, wu, wdu, wib, wub, winst, a.x, a.y, L, cl);
+            relax_arc<ASTAR, AM, IW>(p, s, wu, wdu, wib, wub, winst, a.x, a.y, L, cl);
         }
     }
 }
 
 // Relaxes the selected arcs of the items held by the CTA's threads (at most one
 // item per thread) with the mapping MAP. Called by every thread of the CTA.
-template <bool ASTAR, int AM, int MAP>
+template <bool ASTAR, int AM, int MAP, bool IW = false>
 __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, bool act, u32 u, u32 du,
                                             u32 ib, u64 ub, u32 inst, u32 eb, u32 ee, Local& L, Coop& cs,
                                             Coop* cl, int kind) {
@@ -799,9 +810,9 @@ __device__ __forceinline__ void relax_items(const RunParams& p, const Snap& s, b
         // short rows only: each warp balances its own items; else the CTA does
         // (no CTA vote when no row of the graph has more than 32 arcs)
         if (!p.short_rows && __syncthreads_or(act && ee - eb > WARP_ROW_MAX))
-            relax_chunk_edges<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
+            relax_chunk_edges<ASTAR, AM, IW>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cs, cl);
         else
-            relax_items_warp<ASTAR, AM>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cl);
+            relax_items_warp<ASTAR, AM, IW>(p, s, act, u, du, ib, ub, inst, eb, ee, L, cl);
     }
 }
 
@@ -1383,7 +1394,7 @@ static __device__ __noinline__ void iw_advance(const RunParams& p, const Snap& s
 // Starts a run under independent windows (transition thread, at INIT): every
 // instance's first window [0, Delta), one pending unit each, the sources queued
 // in the ring with distance 0.
-__device__ __forceinline__ void enter_iw(const RunParams& p, Ctl& sc, Rd& r) {
+static __device__ __noinline__ void enter_iw(const RunParams& p, Ctl& sc, Rd& r) {
     const u32 k = p.k;
     const u64 hi = r.delta ? (u64)r.delta : 1ull;
     const u32 fe = r.far_epoch;
@@ -1631,9 +1642,9 @@ __device__ __forceinline__ void inst_drain(const RunParams& p, const Snap& s, Lo
             if (nr) __threadfence();  // the earlier passes' far pushes and state updates first
             for (u32 q = threadIdx.x; q < nr; q += 32u) iw_release(p, sh, sh.rel[q], K, c);
         }
-        relax_items<false, AM, 2>(p, s, act, u, du, ib, w, inst, eb, ee, L, cs, &cs, K_LIGHT);
+        relax_items<false, AM, 2, true>(p, s, act, u, du, ib, w, inst, eb, ee, L, cs, &cs, K_LIGHT);
         if (n > RS)  // block-uniform
-            relax_items<false, AM, 2>(p, s, act2, u2, du2, ib2, w2, inst2, eb2, ee2, L, cs, &cs, K_LIGHT);
+            relax_items<false, AM, 2, true>(p, s, act2, u2, du2, ib2, w2, inst2, eb2, ee2, L, cs, &cs, K_LIGHT);
         __syncthreads();  // every push of the pass has been performed
         if (threadIdx.x < 32u) {
             // entries finished; a hold the CTA no longer needs is marked for release
@@ -2368,13 +2379,6 @@ static __device__ void transition(const RunParams& p, Ctl& sc, u32* s_flag, floa
                            float* act1) {
     const u32 t = threadIdx.x;
     __shared__ u64 s_key0;
-    if (p.policy && p.net) {
-        // the network's 40 KB into this CTA's L1 while the decision's features are
-        // gathered (its layers then read them without an L2 round trip each)
-        const char* w = reinterpret_cast<const char*>(p.net);
-        for (u32 off = t * 128u; off < (u32)sizeof(PolicyNet); off += blockDim.x * 128u)
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(w + off));
-    }
     // s_flag[0]: 0 = no bucket advance, 1 = advance with the policy, 2 = fixed Delta
     if (t == 0) {
         Rd& r = sc.rd;
@@ -2741,9 +2745,10 @@ __device__ __forceinline__ void grid_barrier(const RunParams& p, Snap& s, Local&
 // ---------------------------------------------------------------------------
 // The persistent kernel.
 // ---------------------------------------------------------------------------
-// WD: asynchronous buckets drained by warp workers (hybrid mapping only; its
-// own instantiation, so the block-synchronous drain's code stays as it is).
-template <bool ASTAR, int AM, int MAP, bool WD = false>
+// WD: asynchronous buckets drained by warp workers; IWK: independent bucket
+// windows (hybrid mapping only, SSSP only for IWK; each its own instantiation, so
+// the block-synchronous drain's code and registers stay as they are).
+template <bool ASTAR, int AM, int MAP, bool WD = false, bool IWK = false>
 __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p) {
     __shared__ Snap s;
     // the cooperative-mapping arrays and the claimed list live in dynamic shared
@@ -2756,8 +2761,7 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
     __shared__ float s_feat[POL_IN];
     __shared__ float act0[POL_H], act1[POL_H];
     Local L;
-    // independent bucket windows exist for SSSP with the hybrid mapping's CTA passes
-    constexpr bool IW_KERNEL = !ASTAR && MAP == 2 && !WD;
+    static_assert(!IWK || (!ASTAR && MAP == 2 && !WD), "independent windows: SSSP, hybrid mapping, CTA passes");
     // Failure test: with CTA 0 absent no barrier completes; every other CTA's
     // wait runs into its time limit and the run ends with DS_TIMEOUT.
     if (p.test_absent_cta && blockIdx.x == 0) return;
@@ -2800,8 +2804,8 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
             round_naive<ASTAR, AM>(p, s, L);
         } else if (ph == PH_COMPACT) {
             round_compact(p, s, cs);
-        } else if (ph == PH_ASYNC && IW_KERNEL && p.iw) {
-            if constexpr (IW_KERNEL) inst_drain<AM>(p, s, L, cs);
+        } else if (ph == PH_ASYNC && IWK) {
+            if constexpr (IWK) inst_drain<AM>(p, s, L, cs);
         } else if (ph == PH_ASYNC) {
             if constexpr (WD) wq_reset(cs);
             if (s.in_count) {
@@ -2821,7 +2825,10 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
         grid_barrier(p, s, L, red, sc, s_flag, s_feat, act0, act1);
     }
 
-    // Per-warp reduction of the counters, one atomicAdd per warp.
+    // Counters summed per warp, then per CTA: one atomicAdd per CTA and counter.
+    __shared__ unsigned long long s_st[4];
+    if (threadIdx.x < 4u) s_st[threadIdx.x] = 0ull;
+    __syncthreads();
     unsigned long long a = L.edges, b = L.atomics, cc = L.updates, d = L.pushes;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -2831,12 +2838,13 @@ __global__ void __maxnreg__(64) k_persistent(const __grid_constant__ RunParams p
         d += __shfl_down_sync(FULL, d, o);
     }
     if ((threadIdx.x & 31u) == 0) {
-        unsigned long long* st = p.ctl->stats;
-        if (a) atomicAdd(&st[0], a);
-        if (b) atomicAdd(&st[1], b);
-        if (cc) atomicAdd(&st[2], cc);
-        if (d) atomicAdd(&st[3], d);
+        if (a) atomicAdd(&s_st[0], a);
+        if (b) atomicAdd(&s_st[1], b);
+        if (cc) atomicAdd(&s_st[2], cc);
+        if (d) atomicAdd(&s_st[3], d);
     }
+    __syncthreads();
+    if (threadIdx.x < 4u && s_st[threadIdx.x]) atomicAdd(&p.ctl->stats[threadIdx.x], s_st[threadIdx.x]);
 }
 
 }  // namespace pfg
