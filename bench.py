@@ -443,7 +443,7 @@ def extras(g):
         for K in Ks:
             # the drain kind and launch shape the autotuner chooses between, timed per batch size
             cands = {}
-            # (Auto: a shared window below 128 sources, a window per instance from 128 on)
+            # (Auto: a shared window below 96 sources, a window per instance from 96 on)
             for sched in (Schedule.Auto, Schedule.Warp):
                 for bsz, bps in ((256, 4), (512, 2), (1024, 1)):
                     o = replace(HEADLINE_OPTIONS(), schedule=sched, blockSize=bsz, blocksPerSM=bps)

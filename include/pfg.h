@@ -79,7 +79,7 @@ enum pfg_policy_kind { PFG_POLICY_FIXED = 0, PFG_POLICY_LEARNED = 1 };
  *         policy and block_size >= 64 when Delta >= the largest weight (every
  *         arc light) and no row has more than 8 x block_size arcs; elsewhere it
  *         runs as ASYNC.
- * AUTO:   INSTANCE where it applies to a batch of 128 or more sources
+ * AUTO:   INSTANCE where it applies to a batch of 96 or more sources
  *         (environment PFG_INST_WINDOWS: that threshold, 0 = never), else ASYNC
  *         for Delta-stepping; ROUNDS for Naive and Frontier. */
 enum pfg_schedule { PFG_SCHEDULE_AUTO = 0, PFG_SCHEDULE_ROUNDS = 1, PFG_SCHEDULE_ASYNC = 2,

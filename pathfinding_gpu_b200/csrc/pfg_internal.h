@@ -89,7 +89,7 @@ struct pfg_solver {
     unsigned long long* d_ring = nullptr;  // ring queue of asynchronous buckets [ring_mask + 1], RING_FREE when idle
     u32 ring_mask = 0;
     u32* d_aq = nullptr;        // ring counters [AQ_WORDS]
-    u32* d_iw = nullptr;        // independent-window block [iw_words(K)] (K <= IW_MAX_INST)
+    u32* d_iw = nullptr;        // independent-window block [iw_words(min(K, IW_MAX_INST))]
     pfg::HubRec* d_hubs = nullptr;  // hub records of the grid tier [hub_cap]
     u32 hub_cap = 0;
     u32* d_srcs = nullptr;

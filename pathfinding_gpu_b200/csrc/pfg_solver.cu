@@ -316,7 +316,11 @@ extern "C" pfg_status pfg_create_on_device(const uint32_t* row, const uint32_t* 
     TRYC(cudaMemsetAsync(s->d_aq, 0, AQ_WORDS * 4, s->stream));
     // Independent bucket windows: per-instance windows, pending counts and far-pile
     // counters (every run that uses them rewrites the block first).
-    if (K <= IW_MAX_INST && Kn < (u64)IW_FAR_BIT) TRY(s->dalloc(&s->d_iw, iw_words(K)));
+    // Sized for runs of up to IW_MAX_INST sources whatever maxBatch is (each run checks its own k).
+    {
+        const u32 kw = std::min<u32>(K, IW_MAX_INST);
+        if ((u64)kw * n < (u64)IW_FAR_BIT) TRY(s->dalloc(&s->d_iw, iw_words(kw)));
+    }
     // Hub records: every instance's hub rows once per round, twice over for
     // re-published rows of an asynchronous drain (overflow falls back to the CTA).
     if (s->hub_rows) {
@@ -492,7 +496,7 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     // after the other, so the automatic Delta is widened (4x, PFG_IW_DELTA_MULT): the
     // extra relaxations of wider windows overlap with other instances' work (1000 x 1000
     // grid, 256 sources: 56.9 ms with a shared window at the automatic Delta, 35.9 ms).
-    // The automatic schedule takes them from 128 instances on (PFG_INST_WINDOWS: the
+    // The automatic schedule takes them from 96 instances on (PFG_INST_WINDOWS: the
     // smallest batch, 0 = never), where they measured faster; PFG_SCHEDULE_INSTANCE asks
     // for them at any batch size and falls back to a shared window where they do not apply.
     const u64 iw_delta = o.delta ? (u64)o.delta
@@ -502,7 +506,7 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
                          o.mapping == PFG_MAP_HYBRID && o.policy != PFG_POLICY_LEARNED && !d_trace &&
                          s->max_deg <= 8u * (u32)o.block_size &&
                          o.block_size >= 64;  // (warp 0 of a CTA serves, the others relax)
-    const int iw_min = env_int("PFG_INST_WINDOWS", 128);
+    const int iw_min = env_int("PFG_INST_WINDOWS", 96);
     const bool iw = iw_fits && (o.schedule == PFG_SCHEDULE_INSTANCE ||
                                 (o.schedule == PFG_SCHEDULE_AUTO && iw_min > 0 && (int)k >= iw_min));
     if (iw) delta = (u32)iw_delta;

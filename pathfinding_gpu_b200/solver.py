@@ -53,7 +53,7 @@ class Policy(IntEnum):
 
 class Schedule(IntEnum):
     """How a Delta-stepping bucket is worked off (pfg_schedule in include/pfg.h)."""
-    Auto = 0    # Instance from 128 sources where it applies, else Async for Delta-stepping; Rounds otherwise
+    Auto = 0    # Instance from 96 sources where it applies, else Async for Delta-stepping; Rounds otherwise
     Rounds = 1  # relaxation rounds separated by grid barriers (the reference's loop)
     Async = 2   # one drain per bucket through CTA claimed lists and a ring queue
     Warp = 3    # Async, the drain worked by independent warps (Hybrid mapping)

@@ -134,10 +134,28 @@ def test_instance_windows_grid(oracle, k):
                                                                schedule=Schedule.Instance))
                 _check_batch(oracle, g, srcs, state)
                 assert stats.buckets >= k  # every instance's first window counts
-        # the automatic schedule (independent windows from 128 sources) and a shared window
+        # the automatic schedule (independent windows from 96 sources) and a shared window
         for sched in (Schedule.Auto, Schedule.Async):
             _, _, state = s.run_state(srcs, GpuOptions(schedule=sched))
             _check_batch(oracle, g, srcs, state)
+
+
+def test_instance_windows_at_the_instance_limit(oracle):
+    # 256 instances (the most one run takes with a window each; every CTA holds many of
+    # them at once) and 257 (a shared window): identical results, checked on a sample
+    g = pf.grid(60, 50, SEED + 21)
+    srcs = pf.uniform_vertices(g.n, 257, SEED + 22).tolist()
+    check = [0, 1, 127, 200, 255]
+    with pf.GpuSolver(g, 257) as s:
+        for k in (256, 257):
+            stats, _, state = s.run_state(srcs[:k], GpuOptions(schedule=Schedule.Instance))
+            dist, parent = pf.unpack(state)
+            for i in check:
+                d_ref, p_can = oracle.sssp_canonical(g, srcs[i])
+                assert np.array_equal(dist[i * g.n:(i + 1) * g.n], d_ref), (k, i)
+                assert np.array_equal(parent[i * g.n:(i + 1) * g.n], p_can), (k, i)
+            # a window per instance counts every instance's windows; a shared one its buckets
+            assert (stats.buckets >= k) == (k <= 256), (k, stats.buckets)
 
 
 def test_instance_windows_fallbacks_and_long_rows(oracle, rmat12, rmat12_solver):
