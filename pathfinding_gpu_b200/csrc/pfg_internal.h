@@ -119,6 +119,7 @@ struct pfg_solver {
     int last_mode = pfg::MODE_DELTA;
     u32 last_delta = 0;
     u32 last_k = 0;
+    bool last_iw = false; // the run in flight uses independent bucket windows
     u32 epoch_hint = 1;   // largest epoch known to the host (stamps reset near 2^32)
     std::vector<void*> allocs;
 

@@ -647,6 +647,7 @@ static pfg_status enqueue_run(pfg_solver* s, const uint32_t* h_srcs, const uint3
     s->last_mode = mode;
     s->last_delta = delta;
     s->last_k = k;
+    s->last_iw = iw;
     return PFG_OK;
 }
 
@@ -657,6 +658,10 @@ static pfg_status complete_run(pfg_solver* s, pfg_stats* stats_out) {
     PFG_CUDA(cudaStreamSynchronize(s->stream));
     const Ctl* c = s->h_ctl;
     s->epoch_hint = std::max({c->near_epoch, c->far_epoch, c->r_epoch});
+    // Independent windows advance the far epochs inside the drain and record the last one at
+    // the final transition; a run that failed before it may have left newer stamps, so the
+    // stamp words are cleared before the next run.
+    if (s->last_iw && c->rd.status != DS_OK) s->epoch_hint = 0xFFFFFFFFu;
     if (stats_out) {
         memset(stats_out, 0, sizeof(*stats_out));
         stats_out->edges_scanned = c->stats[0];

@@ -35,6 +35,30 @@ def test_barrier_wait_times_out_and_solver_recovers(oracle, monkeypatch, opt):
             assert np.array_equal(p[i * g.n:(i + 1) * g.n], p_can)
 
 
+def test_instance_windows_run_times_out_and_solver_recovers(oracle, monkeypatch):
+    # a multi-source run under independent windows that fails: the solver clears its stamp
+    # words before the next run (the failed drain may have used far epochs it never recorded)
+    g = pf.grid(40, 40, 3)
+    srcs = [7, 1500, 800]
+    opt = GpuOptions(schedule=Schedule.Instance)
+    with pf.GpuSolver(g, 3) as s:
+        for _ in range(2):
+            _, _, state = s.run_state(srcs, opt)
+        monkeypatch.setenv("PFG_TIMEOUT_MS", "100")
+        monkeypatch.setenv("PFG_TEST_ABSENT_CTA", "1")
+        with pytest.raises(RuntimeError) as e:
+            s.run_state(srcs, opt)
+        assert getattr(e.value, "status", None) == 5, e.value
+        monkeypatch.delenv("PFG_TEST_ABSENT_CTA")
+        for sched in (Schedule.Instance, Schedule.Async, Schedule.Instance):
+            _, _, state = s.run_state(srcs, GpuOptions(schedule=sched))
+            d, p = pf.unpack(state)
+            for i, src in enumerate(srcs):
+                d_ref, p_can = oracle.sssp_canonical(g, src)
+                assert np.array_equal(d[i * g.n:(i + 1) * g.n], d_ref), (sched, i)
+                assert np.array_equal(p[i * g.n:(i + 1) * g.n], p_can), (sched, i)
+
+
 def test_long_progressing_drain_is_not_a_timeout(oracle, monkeypatch):
     # A 100,000-vertex path with one huge bucket: one CTA walks the chain for
     # far longer than the 100 ms wait limit while every other CTA waits. The
