@@ -2334,10 +2334,20 @@ static __device__ void frontier_sample(const RunParams& p, const u32* q, u32 cnt
             r1 = __ldg(p.prow + rb + u + 1);
         }
         const u32 slots = r1 - r0;
+        const u32 d = st_dist(ld_state(p.state + gi));  // (issued with the row's loads)
+        u32 light;
+        if (p.row_stride) {
+            // the row's ROW_ALIGN slots in two 16-byte loads, counted directly
+            const uint4* a4 = reinterpret_cast<const uint4*>(p.adj + r0);
+            const uint4 q0 = __ldg(a4), q1 = __ldg(a4 + 1);
+            light = (q0.y <= delta ? 1u : 0u) + (q0.w <= delta ? 1u : 0u) + (q1.y <= delta ? 1u : 0u) +
+                    (q1.w <= delta ? 1u : 0u);
+        } else {
+            light = light_end(p.adj, r0, r1, delta) - r0;
+        }
         atomicAdd(&s_bin[slots <= 4u ? 0 : (slots <= 32u ? 1 : 2)], 1u);
-        atomicAdd(&s_bin[3], light_end(p.adj, r0, r1, delta) - r0);
+        atomicAdd(&s_bin[3], light);
         atomicAdd(&s_slots, slots);
-        const u32 d = st_dist(ld_state(p.state + gi));
         if (d != INF32) {
             atomicMin(&s_dmin, d);
             atomicMax(&s_dmax, d);
