@@ -134,10 +134,14 @@ def test_instance_windows_grid(oracle, k):
                                                                schedule=Schedule.Instance))
                 _check_batch(oracle, g, srcs, state)
                 assert stats.buckets >= k  # every instance's first window counts
-        # the automatic schedule (independent windows from 96 sources) and a shared window
+        # the automatic schedule (independent windows from 96 sources) and a shared window;
+        # a window per instance counts at least one window per instance, a shared window
+        # far fewer buckets than that on this graph
         for sched in (Schedule.Auto, Schedule.Async):
-            _, _, state = s.run_state(srcs, GpuOptions(schedule=sched))
+            stats, _, state = s.run_state(srcs, GpuOptions(schedule=sched))
             _check_batch(oracle, g, srcs, state)
+            per_instance = sched == Schedule.Auto and k >= 96
+            assert (stats.buckets >= k) == per_instance or k <= 17, (sched, k, stats.buckets)
 
 
 def test_instance_windows_at_the_instance_limit(oracle):
